@@ -1,0 +1,1054 @@
+/*
+ * B200 (sm_100a) backend for the coherent harmonic-sum search.
+ *
+ * Drop-in replacement for the reference GPU backend (src/cuda.cu and the
+ * no-CUDA stub src/gpu_stub.c): it exports the same cs_gpu_* C ABI
+ * (include/coherent_search.h:436-460) and returns the same candidates.  The
+ * reference runs, per chunk of trials, four launches (zero-columns,
+ * interpolation, cuFFT c2r, metric) plus cuFFT + metric per non-divisor
+ * decimation, with the profiles round-tripping through global memory.  Here a
+ * single persistent kernel does all of it per 128-trial tile, on chip:
+ *
+ *   1. interpolation (src/cuda.cu:86-140, src/interp.c:608-824): each thread
+ *      evaluates the m-tap sinc interpolation of 4 consecutive harmonics of
+ *      one trial with the reference's exact FP32 FMA chain and rotation, so
+ *      the harmonic amplitudes are bit-identical to the reference's;
+ *   2. the c2r profile transform (cuFFT C2R in the reference) as a dense
+ *      [128 trials x 2*nharms] x [2*nharms x bins] contraction on the
+ *      5th-generation tensor cores (tcgen05.mma kind::f16, accumulator in
+ *      tensor memory) with a 3-term fp16 split of both operands (hi*hi +
+ *      lo*hi + hi*lo) and a per-run power-of-two scale, which keeps ~22
+ *      significant bits -- FP32-class accuracy;  non-divisor decimations are
+ *      extra output columns of the same MMA;
+ *   3. the boxcar matched filter (src/cuda.cu:164-278, src/boxcar.c:203-252)
+ *      and the k | nharms folds (src/search.c:294-400) read the accumulator
+ *      with tcgen05.ld, in the reference's FP32 expression order;
+ *   4. threshold + warp-ballot compaction of candidate records into a
+ *      device-resident buffer; the host sorts them into the reference's
+ *      (chunk, slot, trial) order and applies its FP64 frequency arithmetic.
+ *
+ * Every wait in the kernel is bounded (an mbarrier poll with a wall-clock
+ * limit); on expiry the kernel records an error, frees its tensor memory and
+ * returns, and the host reports the failure instead of hanging.
+ */
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "cs_internal.h"
+#include "cs_b200.h"
+
+#define CS_EXPORT extern "C" __attribute__((visibility("default")))
+
+#define CS_NTHREADS 256
+#define CS_WAIT_NS 2000000000ull  /* 2 s bound on any in-kernel wait */
+
+/* ------------------------------------------------------------------ */
+/* Kernel arguments                                                   */
+/* ------------------------------------------------------------------ */
+struct SearchArgs {
+    const float2 *amps;
+    long long namps;
+    const CsHarm *harm;
+    const uint16_t *rowtab;
+    const float *W;
+    const float2 *A;
+    const uint8_t *carry;
+    const CsChunk *chunks;
+    const int *tiles;
+    int ntiles;
+    const uint4 *bimg;          /* B hi image then B lo image */
+    int bbytes;                 /* bytes of one B image */
+    int nh, m, q, pnum;
+    unsigned qmagic;
+    int kpad, npad, ncols_tmem;
+    int nslot;
+    CsSlot slot[CS_MAX_SLOT];
+    float gbound;
+    const unsigned *amax;       /* [0]: max |component| bits, [1]: non-finite flag */
+    double thresh;
+    CsRec *recs;
+    unsigned *count;
+    unsigned cap;
+    int *err;
+};
+
+/* ------------------------------------------------------------------ */
+/* PTX helpers (tcgen05, mbarrier, proxy fences)                       */
+/* ------------------------------------------------------------------ */
+static __device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+static __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar), "r"(count));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+static __device__ __forceinline__ uint32_t mbar_try(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+    return ok;
+}
+
+static __device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+/* Bounded wait for the phase with the given parity to complete. */
+static __device__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try(bar, parity)) {
+        if (global_ns() - t0 > CS_WAIT_NS) return false;
+    }
+    return true;
+}
+
+static __device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+static __device__ __forceinline__ void tc_fence_before()
+{
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+static __device__ __forceinline__ void tc_fence_after()
+{
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+static __device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols)
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(dst_smem), "r"(ncols) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+static __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                 :: "r"(taddr), "r"(ncols) : "memory");
+}
+
+/* D[tmem] (+)= A[smem] * B[smem]^T, 128 x N x 16, fp16 in, fp32 accumulate. */
+static __device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t adesc,
+                                               uint64_t bdesc, uint32_t idesc,
+                                               uint32_t accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                 :: "r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+                 : "memory");
+}
+static __device__ __forceinline__ void mma_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(bar) : "memory");
+}
+
+/* 32 consecutive accumulator columns of this warp's 32 lanes. */
+static __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v)
+{
+    uint32_t r[32];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                 "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                   "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                   "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+                   "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                   "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]),
+                   "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+/* Shared-memory matrix descriptor, canonical K-major layout without swizzle:
+ * 8-row x 16-byte core matrices; lbo = byte distance between the two K
+ * halves of one MMA (adjacent K core matrices), sbo = between 8-row groups. */
+static __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;                 /* descriptor version for sm_100 */
+    return d;                                /* base offset 0, no swizzle */
+}
+
+/* floor(u / q) and u mod q for q >= 2 with a precomputed 32-bit multiplier
+ * floor(2^32/q)+1 (the estimate is exact or one too large). */
+static __device__ __forceinline__ void divmod_q(uint32_t u, uint32_t q, uint32_t magic,
+                                                uint32_t &quo, uint32_t &rem)
+{
+    if (q == 1) { quo = u; rem = 0; return; }
+    uint32_t e = __umulhi(u, magic);
+    uint32_t pr = e * q;
+    if (pr > u) { e -= 1; pr -= q; }
+    quo = e;
+    rem = u - pr;
+}
+
+/* ------------------------------------------------------------------ */
+/* Spectrum magnitude bound -> fp16 operand scale                      */
+/* ------------------------------------------------------------------ */
+__global__ void cs_amax_kernel(const float2 *__restrict__ amps, long long namps,
+                               unsigned *__restrict__ out)
+{
+    float mx = 0.0f;
+    unsigned bad = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < namps;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float2 a = amps[i];
+        const float v = fmaxf(fabsf(a.x), fabsf(a.y));
+        if (!(v <= 3.0e38f)) bad = 1;       /* NaN or Inf */
+        mx = fmaxf(mx, v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&out[0], __float_as_uint(mx));
+        if (bad) atomicOr(&out[1], 1u);
+    }
+}
+
+/* 2^e with e chosen so that gbound * amax * 2^e <= 2^14 (fp16 max 65504). */
+static __device__ float operand_scale(const unsigned *amax, float gbound)
+{
+    const float a = __uint_as_float(amax[0]);
+    if (amax[1] != 0u || !(a > 0.0f)) return 1.0f;
+    const float bound = a * gbound;
+    if (!(bound > 0.0f) || !(bound < 3.0e38f)) return 1.0f;
+    int e;
+    frexpf(bound, &e);                      /* bound in [2^(e-1), 2^e) */
+    int s = 14 - e;
+    s = max(-100, min(100, s));
+    return ldexpf(1.0f, s);
+}
+
+/* ------------------------------------------------------------------ */
+/* The fused search kernel                                             */
+/* ------------------------------------------------------------------ */
+struct SmemLayout {
+    int b_off, a_off, ps_off, rk_off, bar_off, tm_off, total;
+};
+
+static __host__ __device__ inline int cs_align(int x, int a) { return (x + a - 1) / a * a; }
+
+/* B images | A images (aliased by the epilogue scratch) | barrier | tmem slot */
+static __host__ __device__ inline SmemLayout smem_layout(int npad, int kpad, int nbmax, int wmaxmax,
+                                                          int nkfold)
+{
+    SmemLayout L;
+    const int bimg = npad * kpad * 2;
+    const int aimg = CS_TILE_M * kpad * 2;
+    L.b_off = 0;
+    L.a_off = cs_align(2 * bimg, 1024);
+    const int ps_bytes = (nbmax + wmaxmax + 1) * CS_TILE_M * 4;
+    const int rk_bytes = nkfold * CS_TILE_M * 4;
+    L.ps_off = L.a_off;
+    L.rk_off = L.ps_off + cs_align(ps_bytes, 128);
+    const int epi_end = L.rk_off + rk_bytes;
+    const int a_end = L.a_off + 2 * aimg;
+    L.bar_off = cs_align(epi_end > a_end ? epi_end : a_end, 16);
+    L.tm_off = L.bar_off + 16;
+    L.total = L.tm_off + 16;
+    return L;
+}
+
+/* Maximum of the sliding-window sums for every width, then the reference
+ * metric max_w (M_w - duty_w * total) * invsw_w (src/boxcar.c:213-231). */
+static __device__ __forceinline__ float scan_widths(const float *ps, int row, int nk,
+                                                    const CsSlot &s, const float *invsw)
+{
+    float mx[CS_NWMAX];
+#pragma unroll
+    for (int w = 0; w < CS_NWMAX; w++) mx[w] = -INFINITY;
+    for (int p = 1; p <= nk; p++) {
+        const float base = ps[(p - 1) * CS_TILE_M + row];
+#pragma unroll
+        for (int w = 0; w < CS_NWMAX; w++) {
+            if (w < s.nw) {
+                const float d = __fsub_rn(ps[(p - 1 + s.widths[w]) * CS_TILE_M + row], base);
+                mx[w] = fmaxf(mx[w], d);
+            }
+        }
+    }
+    const float tot = __fsub_rn(ps[nk * CS_TILE_M + row], ps[row]);
+    float best = -INFINITY;
+#pragma unroll
+    for (int w = 0; w < CS_NWMAX; w++) {
+        if (w < s.nw) {
+            const float c = __fmul_rn(__fsub_rn(mx[w], __fmul_rn(s.duty[w], tot)), invsw[w]);
+            best = fmaxf(best, c);
+        }
+    }
+    return best;
+}
+
+template <int MT>
+__global__ void __launch_bounds__(CS_NTHREADS, 1)
+cs_search_kernel(const SearchArgs args)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const int lane = tid & 31;
+    const int nh = args.nh;
+    const int kpad = args.kpad, npad = args.npad;
+    const int m = MT ? MT : args.m;
+
+    int nbmax = 2 * nh, wmaxmax = 0, nkfold = 0;
+    for (int s = 0; s < args.nslot; s++) {
+        nbmax = max(nbmax, args.slot[s].nk);
+        wmaxmax = max(wmaxmax, args.slot[s].wmax);
+        if (args.slot[s].fold) nkfold = max(nkfold, args.slot[s].nk);
+    }
+    const SmemLayout L = smem_layout(npad, kpad, nbmax, wmaxmax, nkfold);
+    unsigned char *bsm = smem + L.b_off;
+    unsigned char *asm_ = smem + L.a_off;
+    float *ps = reinterpret_cast<float *>(smem + L.ps_off);
+    float *rk = reinterpret_cast<float *>(smem + L.rk_off);
+    const uint32_t bar = smem_u32(smem + L.bar_off);
+    uint32_t *tm_slot = reinterpret_cast<uint32_t *>(smem + L.tm_off);
+    __shared__ CsHarm harm_s[CS_MAX_NH];
+
+    if (warp == 0) tmem_alloc(smem_u32(tm_slot), (uint32_t)args.ncols_tmem);
+    if (tid == 0) mbar_init(bar, 1);
+    for (int h = tid; h < nh; h += blockDim.x) harm_s[h] = args.harm[h];
+    {   /* both B images, verbatim */
+        const int n16 = (2 * args.bbytes) / 16;
+        uint4 *dst = reinterpret_cast<uint4 *>(bsm);
+        for (int i = tid; i < n16; i += blockDim.x) dst[i] = args.bimg[i];
+    }
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tm_slot;
+    const float scale = operand_scale(args.amax, args.gbound);
+    const float inv_scale = 1.0f / scale;    /* exact: power of two */
+
+    const int bimg = args.bbytes;
+    const int aimg = CS_TILE_M * kpad * 2;
+    const uint32_t a_hi = smem_u32(asm_), a_lo = a_hi + (uint32_t)aimg;
+    const uint32_t b_hi = smem_u32(bsm), b_lo = b_hi + (uint32_t)bimg;
+    const uint32_t lbo_a = CS_TILE_M * 16, lbo_b = (uint32_t)npad * 16;
+    const uint32_t idesc = (1u << 4) | ((uint32_t)(npad >> 3) << 17) | ((uint32_t)(CS_TILE_M >> 4) << 24);
+    const int nhb = (nh + 3) / 4;
+    uint32_t phase = 0;
+    bool ok = true;
+
+    for (int tile = blockIdx.x; tile < args.ntiles && ok; tile += gridDim.x) {
+        const int ci = args.tiles[3 * tile + 0];
+        const int j0 = args.tiles[3 * tile + 1];
+        const int cnt = args.tiles[3 * tile + 2];
+        const CsChunk &ch = args.chunks[ci];
+        const unsigned long long filled = ch.filled;
+
+        /* ---- 1. interpolation into the A operand (hi, lo) ---- */
+        {
+            const int r = tid & (CS_TILE_M - 1);
+            const int par = tid >> 7;
+            const bool valid = r < cnt;
+            const long long t = ch.i0 + j0 + r;
+            const long long tp = t * (long long)args.pnum;
+            const long long Q = tp / args.q;
+            const uint32_t R = (uint32_t)(tp - Q * args.q);
+            for (int hb = par; hb < nhb; hb += 2) {
+                uint32_t hi_w[4], lo_w[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int h = 4 * hb + u + 1;
+                    float xr = 0.0f, xi = 0.0f;
+                    if (valid && h <= nh && ((filled >> (h - 1)) & 1ULL)) {
+                        const CsHarm hm = harm_s[h - 1];
+                        uint32_t qd, res;
+                        divmod_q((uint32_t)h * R, (uint32_t)args.q, args.qmagic, qd, res);
+                        const long long qint = (long long)h * Q + qd;
+                        const int ph = args.rowtab[(size_t)(h - 1) * args.q + res];
+                        const int row = hm.woff + ph;
+                        const long long base = hm.rfloor0 + qint + args.carry[row];
+                        const long long b0 = base + 1 - m / 2;
+                        const float *wr = args.W + (size_t)row * m;
+                        float ar = 0.0f, ai = 0.0f;
+                        if (b0 >= 0 && b0 + m <= args.namps) {
+                            const float2 *ap = args.amps + b0;
+                            if (MT) {
+#pragma unroll
+                                for (int i = 0; i < (MT ? MT : 1); i += 4) {
+                                    const float4 w4 = __ldg(reinterpret_cast<const float4 *>(wr + i));
+                                    const float2 a0 = __ldg(ap + i), a1 = __ldg(ap + i + 1);
+                                    const float2 a2 = __ldg(ap + i + 2), a3 = __ldg(ap + i + 3);
+                                    ar = __fmaf_rn(w4.x, a0.x, ar); ai = __fmaf_rn(w4.x, a0.y, ai);
+                                    ar = __fmaf_rn(w4.y, a1.x, ar); ai = __fmaf_rn(w4.y, a1.y, ai);
+                                    ar = __fmaf_rn(w4.z, a2.x, ar); ai = __fmaf_rn(w4.z, a2.y, ai);
+                                    ar = __fmaf_rn(w4.w, a3.x, ar); ai = __fmaf_rn(w4.w, a3.y, ai);
+                                }
+                            } else {
+                                for (int i = 0; i < m; i++) {
+                                    const float w = __ldg(wr + i);
+                                    const float2 a = __ldg(ap + i);
+                                    ar = __fmaf_rn(w, a.x, ar);
+                                    ai = __fmaf_rn(w, a.y, ai);
+                                }
+                            }
+                        } else {
+                            for (int i = 0; i < m; i++) {
+                                const long long idx = b0 + i;
+                                float2 a = make_float2(0.0f, 0.0f);
+                                if (idx >= 0 && idx < args.namps) a = __ldg(args.amps + idx);
+                                const float w = __ldg(wr + i);
+                                ar = __fmaf_rn(w, a.x, ar);
+                                ai = __fmaf_rn(w, a.y, ai);
+                            }
+                        }
+                        const float2 g = __ldg(args.A + row);
+                        xr = __fsub_rn(__fmul_rn(g.x, ar), __fmul_rn(g.y, ai));
+                        xi = __fadd_rn(__fmul_rn(g.x, ai), __fmul_rn(g.y, ar));
+                    }
+                    /* split the scaled amplitude into fp16 hi + lo */
+                    const float sr = xr * scale, si = xi * scale;
+                    const __half hr = __float2half_rn(sr), hi_ = __float2half_rn(si);
+                    const __half lr = __float2half_rn(__fsub_rn(sr, __half2float(hr)));
+                    const __half li = __float2half_rn(__fsub_rn(si, __half2float(hi_)));
+                    hi_w[u] = (uint32_t)__half_as_ushort(hr) | ((uint32_t)__half_as_ushort(hi_) << 16);
+                    lo_w[u] = (uint32_t)__half_as_ushort(lr) | ((uint32_t)__half_as_ushort(li) << 16);
+                }
+                /* K block hb holds harmonics 4hb+1..4hb+4 (Re, Im interleaved) */
+                const uint32_t off = (uint32_t)hb * (CS_TILE_M * 16) + (uint32_t)(r >> 3) * 128 + (uint32_t)(r & 7) * 16;
+                *reinterpret_cast<uint4 *>(asm_ + off) = make_uint4(hi_w[0], hi_w[1], hi_w[2], hi_w[3]);
+                *reinterpret_cast<uint4 *>(asm_ + aimg + off) = make_uint4(lo_w[0], lo_w[1], lo_w[2], lo_w[3]);
+            }
+            /* zero K blocks past 2*nh (kpad padding) */
+            for (int hb = nhb + par; hb < kpad / 8; hb += 2) {
+                const uint32_t off = (uint32_t)hb * (CS_TILE_M * 16) + (uint32_t)(r >> 3) * 128 + (uint32_t)(r & 7) * 16;
+                *reinterpret_cast<uint4 *>(asm_ + off) = make_uint4(0, 0, 0, 0);
+                *reinterpret_cast<uint4 *>(asm_ + aimg + off) = make_uint4(0, 0, 0, 0);
+            }
+        }
+        fence_proxy_async();
+        __syncthreads();
+
+        /* ---- 2. tensor-core c2r: D = Ahi*Bhi + Alo*Bhi + Ahi*Blo ---- */
+        tc_fence_after();
+        if (tid == 0) {
+            const int ksteps = kpad / 16;
+            uint32_t acc = 0;
+            for (int pass = 0; pass < 3; pass++) {
+                const uint32_t abase = (pass == 1) ? a_lo : a_hi;
+                const uint32_t bbase = (pass == 2) ? b_lo : b_hi;
+                for (int s = 0; s < ksteps; s++) {
+                    const uint64_t ad = umma_desc(abase + (uint32_t)s * 2 * lbo_a, lbo_a, 128);
+                    const uint64_t bd = umma_desc(bbase + (uint32_t)s * 2 * lbo_b, lbo_b, 128);
+                    mma_f16(tmem, ad, bd, idesc, acc);
+                    acc = 1;
+                }
+            }
+            mma_commit(bar);
+        }
+        {
+            const bool done = mbar_wait(bar, phase);
+            if (!done && lane == 0) atomicExch(args.err, 1);
+            ok = __syncthreads_and(done) != 0;
+        }
+        if (!ok) {
+            /* give the outstanding MMAs one more bounded wait before the
+             * tensor memory they write is released */
+            mbar_wait(bar, phase);
+            break;
+        }
+        phase ^= 1u;
+        tc_fence_after();
+
+        /* ---- 3. boxcar metrics (warps 0-3 own TMEM lanes 0-127) ---- */
+        if (ok && warp < 4) {
+            const int r = warp * 32 + lane;
+            const bool valid = r < cnt;
+            const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+            float best[CS_MAX_SLOT];
+            const int nb = 2 * nh;
+            float v[32];
+            for (int s = 0; s < args.nslot; s++) {
+                const CsSlot &sl = args.slot[s];
+                const int nk = sl.nk;
+                float p = 0.0f;
+                ps[r] = 0.0f;
+                if (!sl.fold) {
+                    /* profile columns col0 .. col0+nk-1, then the wrap */
+                    for (int c0 = 0; c0 < nk; c0 += 32) {
+                        tmem_ld32(trow + (uint32_t)(sl.col0 + c0), v);
+#pragma unroll
+                        for (int u = 0; u < 32; u++) {
+                            if (c0 + u < nk) {
+                                p = __fadd_rn(p, v[u] * inv_scale);
+                                ps[(c0 + u + 1) * CS_TILE_M + r] = p;
+                            }
+                        }
+                    }
+                    for (int c0 = 0; c0 < sl.wmax; c0 += 32) {
+                        tmem_ld32(trow + (uint32_t)(sl.col0 + c0), v);
+#pragma unroll
+                        for (int u = 0; u < 32; u++) {
+                            if (c0 + u < sl.wmax) {
+                                p = __fadd_rn(p, v[u] * inv_scale);
+                                ps[(nk + c0 + u + 1) * CS_TILE_M + r] = p;
+                            }
+                        }
+                    }
+                } else {
+                    /* r_k[j] = (x[j] + x[j+nk] + ...) * (1/k), then prefix */
+                    int jj = 0;
+                    for (int c0 = 0; c0 < nb; c0 += 32) {
+                        tmem_ld32(trow + (uint32_t)c0, v);
+#pragma unroll
+                        for (int u = 0; u < 32; u++) {
+                            const int i = c0 + u;
+                            if (i < nb) {
+                                const float x = v[u] * inv_scale;
+                                if (i < nk) rk[jj * CS_TILE_M + r] = x;
+                                else rk[jj * CS_TILE_M + r] = __fadd_rn(rk[jj * CS_TILE_M + r], x);
+                                jj = (jj + 1 == nk) ? 0 : jj + 1;
+                            }
+                        }
+                    }
+                    const float invk = 1.0f / (float)sl.k;
+                    for (int j = 0; j < nk; j++) {
+                        const float x = __fmul_rn(rk[j * CS_TILE_M + r], invk);
+                        p = __fadd_rn(p, x);
+                        ps[(j + 1) * CS_TILE_M + r] = p;
+                    }
+                    for (int u = 0; u < sl.wmax; u++) {
+                        const float x = __fmul_rn(rk[u * CS_TILE_M + r], invk);
+                        p = __fadd_rn(p, x);
+                        ps[(nk + u + 1) * CS_TILE_M + r] = p;
+                    }
+                }
+                best[s] = scan_widths(ps, r, nk, sl, ch.invsw[s]);
+            }
+            /* ---- 4. threshold + warp-aggregated compaction ---- */
+            const int j = j0 + r;
+            for (int s = 0; s < args.nslot; s++) {
+                const bool hit = valid && j < ch.nvalid[s] && (double)best[s] > args.thresh;
+                const unsigned mask = __ballot_sync(0xffffffffu, hit);
+                if (mask) {
+                    unsigned basei = 0;
+                    if (lane == 0) basei = atomicAdd(args.count, (unsigned)__popc(mask));
+                    basei = __shfl_sync(0xffffffffu, basei, 0);
+                    if (hit) {
+                        const unsigned pos = basei + (unsigned)__popc(mask & ((1u << lane) - 1u));
+                        if (pos < args.cap) {
+                            CsRec rec;
+                            rec.chunk = ci;
+                            rec.slot = s;
+                            rec.j = j;
+                            rec.metric = best[s];
+                            args.recs[pos] = rec;
+                        }
+                    }
+                }
+            }
+        }
+        tc_fence_before();
+        __syncthreads();
+    }
+
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, (uint32_t)args.ncols_tmem);
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* Host side                                                          */
+/* ------------------------------------------------------------------ */
+#define CK(call)                                                               \
+    do {                                                                       \
+        cudaError_t e_ = (call);                                               \
+        if (e_ != cudaSuccess) {                                               \
+            fprintf(stderr, "Error: CUDA %s failed: %s (%s:%d)\n", #call,       \
+                    cudaGetErrorString(e_), __FILE__, __LINE__);               \
+            goto fail;                                                         \
+        }                                                                      \
+    } while (0)
+
+struct GpuSession {
+    const SearchParams *p;
+    int device;
+    int Nprof;
+    long long total, nchunks;
+    long long N, namps;
+    double T, r_lo, lodr;
+    CsTables tab;
+    int max_smem;
+    int nsm;
+    cudaStream_t st;
+    cudaEvent_t ev0, ev1;
+    /* device buffers */
+    float2 *d_amps;
+    CsHarm *d_harm;
+    uint16_t *d_rowtab;
+    float *d_W;
+    float2 *d_A;
+    uint8_t *d_carry;
+    CsChunk *d_chunks;
+    int *d_tiles;
+    uint4 *d_bimg;
+    int bbytes;
+    unsigned *d_amax;      /* [2] */
+    unsigned *d_count;     /* [1] */
+    int *d_err;            /* [1] */
+    CsRec *d_recs;
+    unsigned cap;
+    unsigned *h_count;     /* pinned */
+    float last_kernel_ms;
+    int own_plans;
+};
+
+static cudaError_t select_device(int device)
+{
+    int cur = -1;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e == cudaSuccess && cur == device) return cudaSuccess;
+    return cudaSetDevice(device);
+}
+
+CS_EXPORT int cs_gpu_available(int device, char *errbuf, size_t errlen)
+{
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count <= 0) {
+        if (errbuf) snprintf(errbuf, errlen, "no CUDA device available (%s)",
+                             e != cudaSuccess ? cudaGetErrorString(e) : "0 devices");
+        return -1;
+    }
+    if (device < 0 || device >= count) {
+        if (errbuf) snprintf(errbuf, errlen, "CUDA device %d requested but %d device(s) present",
+                             device, count);
+        return -1;
+    }
+    e = select_device(device);
+    if (e != cudaSuccess) {
+        if (errbuf) snprintf(errbuf, errlen, "cannot select CUDA device %d: %s", device,
+                             cudaGetErrorString(e));
+        return -1;
+    }
+    cudaDeviceProp prop;
+    e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) {
+        if (errbuf) snprintf(errbuf, errlen, "cudaGetDeviceProperties failed: %s",
+                             cudaGetErrorString(e));
+        return -1;
+    }
+    if (prop.major != 10) {
+        if (errbuf) snprintf(errbuf, errlen, "%s (device %d, cc %d.%d) is not an sm_100 "
+                             "(B200-class) device", prop.name, device, prop.major, prop.minor);
+        return -1;
+    }
+    if (errbuf) snprintf(errbuf, errlen, "%s (device %d, cc %d.%d)", prop.name, device,
+                         prop.major, prop.minor);
+    return 1;
+}
+
+static void session_release(GpuSession *S)
+{
+    if (!S) return;
+    cudaFree(S->d_amps);
+    cudaFree(S->d_harm);
+    cudaFree(S->d_rowtab);
+    cudaFree(S->d_W);
+    cudaFree(S->d_A);
+    cudaFree(S->d_carry);
+    cudaFree(S->d_chunks);
+    cudaFree(S->d_tiles);
+    cudaFree(S->d_bimg);
+    cudaFree(S->d_amax);
+    cudaFree(S->d_count);
+    cudaFree(S->d_err);
+    cudaFree(S->d_recs);
+    if (S->h_count) cudaFreeHost(S->h_count);
+    if (S->ev0) cudaEventDestroy(S->ev0);
+    if (S->ev1) cudaEventDestroy(S->ev1);
+    if (S->st) cudaStreamDestroy(S->st);
+    cs_tables_free(&S->tab);
+    free(S);
+}
+
+static int smem_bytes(const CsTables &t)
+{
+    int nbmax = 2 * t.nh, wmaxmax = 0, nkfold = 0;
+    for (int s = 0; s < t.nslot; s++) {
+        nbmax = std::max(nbmax, t.slot[s].nk);
+        wmaxmax = std::max(wmaxmax, t.slot[s].wmax);
+        if (t.slot[s].fold) nkfold = std::max(nkfold, t.slot[s].nk);
+    }
+    return smem_layout(t.npad, t.kpad, nbmax, wmaxmax, nkfold).total;
+}
+
+/* Tensor-memory columns: the accumulator plus whole 32-column loads past
+ * the start of every profile, rounded to a power of two (>= 32). */
+static int tmem_columns(const CsTables &t)
+{
+    int need = t.npad;
+    for (int s = 0; s < t.nslot; s++) {
+        const int c0 = t.slot[s].fold ? 0 : t.slot[s].col0;
+        const int len = t.slot[s].fold ? 2 * t.nh : t.slot[s].nk;
+        need = std::max(need, c0 + (len + 31) / 32 * 32);
+    }
+    int nc = 32;
+    while (nc < need) nc <<= 1;
+    return nc;
+}
+
+static int grow_records(GpuSession *S, unsigned cap)
+{
+    cudaFree(S->d_recs);
+    S->d_recs = NULL;
+    S->cap = 0;
+    if (cudaMalloc((void **)&S->d_recs, (size_t)cap * sizeof(CsRec)) != cudaSuccess) {
+        fprintf(stderr, "Error: cannot allocate %u candidate records on the GPU\n", cap);
+        return -1;
+    }
+    S->cap = cap;
+    return 0;
+}
+
+CS_EXPORT GpuSession *cs_gpu_session_create(const FFTFile *ft, const SearchParams *p,
+                                            const DirectPlanSet *dplans,
+                                            const long long *cstarts, long long total,
+                                            int Nprof, long long nchunks, double r_lo,
+                                            double lodr, int device)
+{
+    char err[512] = {0};
+    GpuSession *S = (GpuSession *)calloc(1, sizeof(GpuSession));
+    std::vector<uint16_t> bhi, blo;
+    size_t img_halves = 0;
+    int smem = 0;
+    if (!S) return NULL;
+    S->p = p;
+    S->device = device;
+    S->Nprof = Nprof;
+    S->total = total;
+    S->nchunks = nchunks;
+    S->N = ft->N;
+    S->namps = ft->namps;
+    S->T = ft->T;
+    S->r_lo = r_lo;
+    S->lodr = lodr;
+    if (cs_tables_build(&S->tab, ft, p, dplans, cstarts, total, nchunks, r_lo, lodr,
+                        err, sizeof(err)) != 0) {
+        fprintf(stderr, "Error: B200 search session: %s\n", err);
+        session_release(S);
+        return NULL;
+    }
+    CK(select_device(device));
+    {
+        cudaDeviceProp prop;
+        CK(cudaGetDeviceProperties(&prop, device));
+        S->max_smem = (int)prop.sharedMemPerBlockOptin;
+        S->nsm = prop.multiProcessorCount;
+    }
+    smem = smem_bytes(S->tab);
+    if (smem > S->max_smem) {
+        fprintf(stderr, "Error: B200 search kernel needs %d bytes of shared memory, device "
+                        "%d allows %d\n", smem, device, S->max_smem);
+        session_release(S);
+        return NULL;
+    }
+    CK(cudaStreamCreateWithFlags(&S->st, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&S->ev0));
+    CK(cudaEventCreate(&S->ev1));
+    CK(cudaMalloc((void **)&S->d_amps, (size_t)(S->namps > 0 ? S->namps : 1) * sizeof(float2)));
+    CK(cudaMalloc((void **)&S->d_harm, sizeof(CsHarm) * CS_MAX_NH));
+    CK(cudaMemcpy(S->d_harm, S->tab.harm, sizeof(CsHarm) * CS_MAX_NH, cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void **)&S->d_rowtab, (size_t)S->tab.nh * S->tab.q * sizeof(uint16_t)));
+    CK(cudaMemcpy(S->d_rowtab, S->tab.rowtab, (size_t)S->tab.nh * S->tab.q * sizeof(uint16_t),
+                  cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void **)&S->d_W, (size_t)S->tab.nrows * S->tab.m * sizeof(float)));
+    CK(cudaMemcpy(S->d_W, S->tab.W, (size_t)S->tab.nrows * S->tab.m * sizeof(float),
+                  cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void **)&S->d_A, (size_t)S->tab.nrows * sizeof(float2)));
+    CK(cudaMemcpy(S->d_A, S->tab.A, (size_t)S->tab.nrows * sizeof(float2), cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void **)&S->d_carry, (size_t)S->tab.nrows));
+    CK(cudaMemcpy(S->d_carry, S->tab.carry, (size_t)S->tab.nrows, cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void **)&S->d_chunks, (size_t)(nchunks > 0 ? nchunks : 1) * sizeof(CsChunk)));
+    if (nchunks > 0)
+        CK(cudaMemcpy(S->d_chunks, S->tab.chunks, (size_t)nchunks * sizeof(CsChunk),
+                      cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void **)&S->d_tiles, (size_t)(S->tab.ntiles > 0 ? S->tab.ntiles : 1) * 3 * sizeof(int)));
+    if (S->tab.ntiles > 0)
+        CK(cudaMemcpy(S->d_tiles, S->tab.tiles, (size_t)S->tab.ntiles * 3 * sizeof(int),
+                      cudaMemcpyHostToDevice));
+    img_halves = (size_t)S->tab.npad * S->tab.kpad;
+    bhi.resize(img_halves);
+    blo.resize(img_halves);
+    cs_tables_dft_images(&S->tab, bhi.data(), blo.data());
+    S->bbytes = (int)(img_halves * 2);
+    CK(cudaMalloc((void **)&S->d_bimg, (size_t)2 * S->bbytes));
+    CK(cudaMemcpy(S->d_bimg, bhi.data(), (size_t)S->bbytes, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((char *)S->d_bimg + S->bbytes, blo.data(), (size_t)S->bbytes,
+                  cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void **)&S->d_amax, 2 * sizeof(unsigned)));
+    CK(cudaMalloc((void **)&S->d_count, sizeof(unsigned)));
+    CK(cudaMalloc((void **)&S->d_err, sizeof(int)));
+    CK(cudaMallocHost((void **)&S->h_count, 4 * sizeof(unsigned)));
+    {
+        /* Start with room for 1 in 16 trials per slot; grown on overflow. */
+        long long want = (total * S->tab.nslot) / 16 + 4096;
+        if (want > (long long)0x7fffffff) want = 0x7fffffff;
+        if (grow_records(S, (unsigned)want) != 0) { session_release(S); return NULL; }
+    }
+    CK(cudaFuncSetAttribute(cs_search_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CK(cudaFuncSetAttribute(cs_search_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return S;
+fail:
+    session_release(S);
+    return NULL;
+}
+
+CS_EXPORT int cs_gpu_session_matches(const GpuSession *S, const FFTFile *ft,
+                                     const SearchParams *p, int Nprof, long long total,
+                                     double r_lo, double lodr, int device)
+{
+    if (!S) return 0;
+    return S->p == p && S->device == device && S->Nprof == Nprof && S->total == total &&
+           S->T == ft->T && S->N == ft->N && S->namps == ft->namps && S->r_lo == r_lo &&
+           S->lodr == lodr;
+}
+
+static SearchArgs make_args(GpuSession *S, const float2 *d_amps, double threshold)
+{
+    SearchArgs a;
+    memset(&a, 0, sizeof(a));
+    const CsTables &t = S->tab;
+    a.amps = d_amps;
+    a.namps = S->namps;
+    a.harm = S->d_harm;
+    a.rowtab = S->d_rowtab;
+    a.W = S->d_W;
+    a.A = S->d_A;
+    a.carry = S->d_carry;
+    a.chunks = S->d_chunks;
+    a.tiles = S->d_tiles;
+    a.ntiles = t.ntiles;
+    a.bimg = S->d_bimg;
+    a.bbytes = S->bbytes;
+    a.nh = t.nh;
+    a.m = t.m;
+    a.q = t.q;
+    a.pnum = t.pnum;
+    a.qmagic = t.q >= 2 ? (uint32_t)(0x100000000ULL / (unsigned long long)t.q + 1ULL) : 0u;
+    a.kpad = t.kpad;
+    a.npad = t.npad;
+    a.ncols_tmem = tmem_columns(t);
+    a.nslot = t.nslot;
+    memcpy(a.slot, t.slot, sizeof(a.slot));
+    a.gbound = t.gbound;
+    a.amax = S->d_amax;
+    a.thresh = threshold;
+    a.recs = S->d_recs;
+    a.count = S->d_count;
+    a.cap = S->cap;
+    a.err = S->d_err;
+    return a;
+}
+
+/* Enqueue the search of the spectrum at d_amps on S->st (no host sync). */
+static cudaError_t enqueue_search(GpuSession *S, const float2 *d_amps, double threshold,
+                                  bool timed)
+{
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(S->d_amax, 0, 2 * sizeof(unsigned), S->st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(S->d_count, 0, sizeof(unsigned), S->st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(S->d_err, 0, sizeof(int), S->st)) != cudaSuccess) return e;
+    if (S->namps > 0) {
+        int g = (int)std::min<long long>((S->namps + 255) / 256, (long long)S->nsm * 8);
+        cs_amax_kernel<<<g, 256, 0, S->st>>>(d_amps, S->namps, S->d_amax);
+    }
+    if (S->tab.ntiles <= 0) return cudaGetLastError();
+    const SearchArgs a = make_args(S, d_amps, threshold);
+    const int smem = smem_bytes(S->tab);
+    const int grid = std::min(S->tab.ntiles, S->nsm);
+    if (timed) cudaEventRecord(S->ev0, S->st);
+    if (S->tab.m == 16)
+        cs_search_kernel<16><<<grid, CS_NTHREADS, smem, S->st>>>(a);
+    else
+        cs_search_kernel<0><<<grid, CS_NTHREADS, smem, S->st>>>(a);
+    if (timed) cudaEventRecord(S->ev1, S->st);
+    return cudaGetLastError();
+}
+
+/* Read back the records and build the candidate list. */
+static int collect(GpuSession *S, double threshold, CandidateList *out, int *need_rerun)
+{
+    *need_rerun = 0;
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(S->h_count, S->d_count, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                             S->st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(S->h_count + 1, S->d_err, sizeof(int), cudaMemcpyDeviceToHost,
+                             S->st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(S->st)) != cudaSuccess) {
+        fprintf(stderr, "Error: B200 search failed: %s\n", cudaGetErrorString(e));
+        return -1;
+    }
+    if (S->h_count[1] != 0) {
+        fprintf(stderr, "Error: B200 search kernel timed out waiting for the tensor cores\n");
+        return -1;
+    }
+    const unsigned n = S->h_count[0];
+    if (n > S->cap) {
+        if (grow_records(S, n + n / 8 + 1024) != 0) return -1;
+        *need_rerun = 1;
+        return 0;
+    }
+    if (n == 0) return 0;
+    std::vector<CsRec> recs(n);
+    if ((e = cudaMemcpy(recs.data(), S->d_recs, (size_t)n * sizeof(CsRec),
+                        cudaMemcpyDeviceToHost)) != cudaSuccess) {
+        fprintf(stderr, "Error: B200 search readback failed: %s\n", cudaGetErrorString(e));
+        return -1;
+    }
+    cs_sort_records(recs.data(), (long long)n);
+    cs_harvest(&S->tab, recs.data(), (long long)n, S->r_lo, S->lodr, (double)S->N, S->T,
+               threshold, out);
+    return 0;
+}
+
+CS_EXPORT CandidateList cs_gpu_session_run(GpuSession *S, const FFTFile *ft, double threshold)
+{
+    CandidateList cands;
+    candlist_init(&cands);
+    if (!S) return cands;
+    if (ft->namps != S->namps || ft->N != S->N) {
+        fprintf(stderr, "Error: GPU session built for N=%lld/%lld amps but the input has "
+                        "N=%lld/%lld\n", S->N, S->namps, ft->N, ft->namps);
+        return cands;
+    }
+    if (select_device(S->device) != cudaSuccess) return cands;
+    if (S->namps > 0) {
+        cudaError_t e = cudaMemcpyAsync(S->d_amps, ft->amps, (size_t)S->namps * sizeof(float2),
+                                        cudaMemcpyHostToDevice, S->st);
+        if (e != cudaSuccess) {
+            fprintf(stderr, "Error: spectrum upload failed: %s\n", cudaGetErrorString(e));
+            return cands;
+        }
+    }
+    for (int attempt = 0; attempt < 2; attempt++) {
+        cudaError_t e = enqueue_search(S, S->d_amps, threshold, false);
+        if (e != cudaSuccess) {
+            fprintf(stderr, "Error: B200 search launch failed: %s\n", cudaGetErrorString(e));
+            return cands;
+        }
+        int rerun = 0;
+        if (collect(S, threshold, &cands, &rerun) != 0) {
+            candlist_free(&cands);
+            return cands;
+        }
+        if (!rerun) break;
+    }
+    return cands;
+}
+
+CS_EXPORT void cs_gpu_session_free(GpuSession *S)
+{
+    if (!S) return;
+    select_device(S->device);
+    cudaStreamSynchronize(S->st);
+    session_release(S);
+}
+
+CS_EXPORT CandidateList cs_gpu_search_region(const FFTFile *ft, const SearchParams *p,
+                                             const DirectPlanSet *dplans,
+                                             const long long *cstarts, long long total,
+                                             int Nprof, long long nchunks, double r_lo,
+                                             double r_hi, double lodr, double threshold,
+                                             int device)
+{
+    (void)r_hi;
+    CandidateList c;
+    candlist_init(&c);
+    GpuSession *S = cs_gpu_session_create(ft, p, dplans, cstarts, total, Nprof, nchunks,
+                                          r_lo, lodr, device);
+    if (!S) return c;
+    c = cs_gpu_session_run(S, ft, threshold);
+    cs_gpu_session_free(S);
+    return c;
+}
+
+/* ------------------------------------------------------------------ */
+/* Additions (cs_b200.h)                                               */
+/* ------------------------------------------------------------------ */
+CS_EXPORT int cs_b200_session_info(const GpuSession *S, CsB200Info *info)
+{
+    if (!S || !info) return -1;
+    memset(info, 0, sizeof(*info));
+    info->ntiles = S->tab.ntiles;
+    info->nchunks = S->tab.nchunks;
+    info->nslot = S->tab.nslot;
+    info->npad = S->tab.npad;
+    info->kpad = S->tab.kpad;
+    info->smem_bytes = smem_bytes(S->tab);
+    info->grid = std::min(S->tab.ntiles, S->nsm);
+    info->total = S->total;
+    info->rec_capacity = S->cap;
+    return 0;
+}
+
+CS_EXPORT int cs_b200_session_enqueue_device(GpuSession *S, const float *d_amps,
+                                             double threshold, void *stream)
+{
+    if (!S) return -1;
+    (void)stream;
+    cudaError_t e = enqueue_search(S, d_amps ? (const float2 *)d_amps : S->d_amps, threshold,
+                                   true);
+    return e == cudaSuccess ? 0 : -1;
+}
+
+CS_EXPORT int cs_b200_session_collect(GpuSession *S, double threshold, CandidateList *out,
+                                      float *kernel_ms)
+{
+    if (!S || !out) return -1;
+    candlist_init(out);
+    int rerun = 0;
+    if (collect(S, threshold, out, &rerun) != 0) return -1;
+    if (kernel_ms) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, S->ev0, S->ev1);
+        *kernel_ms = ms;
+    }
+    return rerun ? 1 : 0;
+}
+
+CS_EXPORT float *cs_b200_session_device_amps(GpuSession *S)
+{
+    return S ? (float *)S->d_amps : NULL;
+}
+
+CS_EXPORT int cs_b200_session_sync(GpuSession *S)
+{
+    if (!S) return -1;
+    return cudaStreamSynchronize(S->st) == cudaSuccess ? 0 : -1;
+}

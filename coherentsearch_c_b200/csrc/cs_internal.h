@@ -1,0 +1,105 @@
+/*
+ * Internal layout shared by the host table builder (host/cs_tables.c, plain
+ * C compiled with -ffp-contract=off so its FP64 arithmetic matches the
+ * reference's) and the CUDA backend (cs_gpu.cu).  Not a public interface.
+ */
+#ifndef CS_INTERNAL_H
+#define CS_INTERNAL_H
+
+#include <stdint.h>
+#include "coherent_search.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CS_TILE_M 128          /* trials per tile = tcgen05 M */
+#define CS_MAX_NH 60           /* harmonics supported by the fused kernel */
+#define CS_MAX_SLOT 8          /* base + decimations */
+#define CS_NWMAX 12            /* boxcar widths per decimation */
+#define CS_MAX_NCOL 256        /* DFT output columns (one MMA, N <= 256) */
+
+/* One decimation slot: slot 0 is the full-resolution profile (k = 1). */
+typedef struct {
+    int k, Hk, nk;             /* factor, harmonics, profile bins (2*Hk) */
+    int fold;                  /* k | nharms: folded from the base profile */
+    int col0;                  /* first DFT column (non-fold slots and base) */
+    int nw, wmax;
+    int widths[CS_NWMAX];
+    float duty[CS_NWMAX];      /* (float)w / (float)nk, src/boxcar.c:220 */
+} CsSlot;
+
+/* One chunk of the reference chunk table (src/interp.c:944-966). */
+typedef struct {
+    long long i0;              /* first trial */
+    int n;                     /* trials */
+    int tile0;                 /* first tile of this chunk */
+    unsigned long long filled; /* bit h-1: harmonic h interpolated */
+    int nvalid[CS_MAX_SLOT];   /* trials below the decimated Nyquist */
+    float invsw[CS_MAX_SLOT][CS_NWMAX];  /* (float)(invsigma * shape[w]) */
+} CsChunk;
+
+/* Device-side per-harmonic table header. */
+typedef struct {
+    long long rfloor0;
+    int P;                     /* phase-cycle length */
+    int woff;                  /* first row in the packed W/A/carry tables */
+} CsHarm;
+
+/* Candidate record written by the kernel. */
+typedef struct {
+    int chunk;
+    int slot;
+    int j;                     /* trial offset inside the chunk */
+    float metric;
+} CsRec;
+
+/* Everything the host builds once per session geometry. */
+typedef struct {
+    int nh, m, q, pnum;
+    int nslot;
+    CsSlot slot[CS_MAX_SLOT];
+    int ncol;                  /* DFT columns used */
+    int npad;                  /* MMA N (multiple of 16) */
+    int kpad;                  /* MMA K (multiple of 16) = 2*nh rounded up */
+    long long nchunks;
+    CsChunk *chunks;           /* nchunks */
+    int ntiles;
+    int *tiles;                /* 3 ints per tile: chunk, j0, count */
+    /* packed interpolation tables */
+    CsHarm harm[CS_MAX_NH];
+    int nrows;                 /* sum of P over harmonics */
+    float *W;                  /* nrows * m */
+    float *A;                  /* nrows * 2 (re, im) */
+    uint8_t *carry;            /* nrows */
+    uint16_t *rowtab;          /* nh * q: residue -> phase index */
+    float gbound;              /* max over rows of (|A_re|+|A_im|) * sum|W| */
+} CsTables;
+
+/* Build / free the tables.  Returns 0 or -1 with a message in err. */
+int  cs_tables_build(CsTables *t, const FFTFile *ft, const SearchParams *p,
+                     const DirectPlanSet *dplans, const long long *cstarts,
+                     long long total, long long nchunks, double r_lo,
+                     double lodr, char *err, size_t errlen);
+void cs_tables_free(CsTables *t);
+
+/* Fill the B operand images (fp16 hi and lo parts of the c2r matrix) in the
+ * canonical no-swizzle K-major UMMA layout: npad rows (output columns) by
+ * kpad (interleaved Re/Im of harmonics 1..nh).  Each image holds
+ * npad*kpad halves, returned as raw 16-bit patterns. */
+void cs_tables_dft_images(const CsTables *t, uint16_t *bhi, uint16_t *blo);
+
+/* Turn sorted records into the reference's Candidate list
+ * (src/cuda.cu:837-881 arithmetic). */
+void cs_harvest(const CsTables *t, const CsRec *recs, long long n,
+                double r_lo, double lodr, double N, double T,
+                double threshold, CandidateList *out);
+
+/* Sort records by (chunk, slot, j). */
+void cs_sort_records(CsRec *recs, long long n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

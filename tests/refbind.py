@@ -1,0 +1,176 @@
+"""Test-side bindings of the checkers under oracle/:
+
+* libcsref.so     -- the reference's own CPU search path (src/*.c compiled
+                     unmodified by oracle/Makefile against the FFTW-API shim)
+* libcsoracle.so  -- oracle/cs_oracle.c, the per-trial CPU restatement
+* libdedisp_ref.so -- the reference's vendored PRESTO dispersion.c
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use these.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from coherentsearch_c_b200 import native as nt
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+_REF = None
+_ORA = None
+
+
+def have_ref() -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "libcsref.so"))
+
+
+def ref_lib() -> C.CDLL:
+    global _REF
+    if _REF is None:
+        lib = nt.declare_host_api(C.CDLL(os.path.join(REF_DIR, "libcsref.so")))
+        lib.datpipe_create.argtypes = [C.c_int, C.c_int, C.c_double]
+        lib.datpipe_create.restype = C.c_void_p
+        lib.datpipe_free.argtypes = [C.c_void_p]
+        lib.datpipe_redfft_mem.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_longlong,
+                                           C.c_double, C.c_char_p, C.POINTER(nt.FFTFile)]
+        lib.datpipe_redfft_mem.restype = C.c_int
+        lib.search_cache_free.argtypes = [C.c_void_p]
+        _REF = lib
+    return _REF
+
+
+def oracle_lib() -> C.CDLL:
+    global _ORA
+    if _ORA is None:
+        lib = C.CDLL(os.path.join(REF_DIR, "libcsoracle.so"))
+        lib.cso_trial_metrics.argtypes = [
+            C.POINTER(C.c_float), C.c_longlong, C.c_longlong, C.c_int, C.c_int, C.c_double,
+            C.c_int, C.POINTER(C.c_int), C.c_double, C.c_double, C.c_double,
+            C.POINTER(C.c_longlong), C.c_longlong, C.c_longlong, C.c_longlong, C.c_int,
+            C.c_int, C.POINTER(C.c_double)]
+        lib.cso_trial_metrics.restype = C.c_int
+        lib.cso_trial_profile.argtypes = [
+            C.POINTER(C.c_float), C.c_longlong, C.c_longlong, C.c_int, C.c_int, C.c_double,
+            C.c_double, C.POINTER(C.c_longlong), C.c_longlong, C.c_longlong, C.c_longlong,
+            C.POINTER(C.c_double)]
+        lib.cso_trial_profile.restype = C.c_int
+        _ORA = lib
+    return _ORA
+
+
+def ref_spectrum(x: np.ndarray, dt: float) -> np.ndarray:
+    """The reference's in-memory realfft + rednoise (src/datpipe.c:417-448)."""
+    lib = ref_lib()
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    pipe = lib.datpipe_create(6, 100, 6.0)
+    ft = nt.FFTFile()
+    rc = lib.datpipe_redfft_mem(pipe, x.ctypes.data_as(C.POINTER(C.c_float)), x.size, dt,
+                                b"mem", C.byref(ft))
+    if rc != 0:
+        lib.datpipe_free(pipe)
+        raise RuntimeError("datpipe_redfft_mem failed")
+    amps = np.ctypeslib.as_array(ft.amps, shape=(2 * ft.namps,)).copy()
+    lib.datpipe_free(pipe)
+    return amps
+
+
+def make_file(amps: np.ndarray, N: int, dt: float) -> nt.FFTFile:
+    ft = nt.FFTFile()
+    ft.amps = amps.ctypes.data_as(C.POINTER(C.c_float))
+    ft.namps = amps.size // 2
+    ft.N = N
+    ft.T = N * dt
+    ft.df = 1.0 / ft.T
+    ft.inf.N = N
+    ft.inf.has_N = 1
+    ft.inf.dt = dt
+    ft.inf.has_dt = 1
+    return ft
+
+
+def ref_search(amps: np.ndarray, N: int, dt: float, opts, precision: int = 0,
+               collapse: bool = True) -> np.ndarray:
+    """The reference CPU search_file (src/search.c:1247) on this spectrum."""
+    lib = ref_lib()
+    ft = make_file(amps, N, dt)
+    p = opts.params(lib)
+    p.precision = precision
+    rem = int(opts.remove) if collapse else 0
+    hrem = int(opts.harm_remove) if collapse else 0
+    cl = lib.search_file(C.byref(ft), C.byref(p), opts.lofreq, opts.hifreq, opts.lobin,
+                         opts.blocksize, opts.threshold, rem, opts.drtol, hrem, opts.numharm,
+                         None, 0, 0, 0, None, None, 1.0, -1)
+    out = nt.candidates_to_numpy(cl)
+    lib.candlist_free(C.byref(cl))
+    return out
+
+
+def ref_chunks(amps: np.ndarray, N: int, dt: float, opts):
+    """(r_lo, lodr, total, cstarts) from the reference planner."""
+    lib = ref_lib()
+    ft = make_file(amps, N, dt)
+    p = opts.params(lib)
+    r_lo, lodr, total = opts.geometry(N, dt)
+    plans = nt.DirectPlanSet()
+    assert lib.direct_plans_build(C.byref(plans), C.byref(p), r_lo) == 0
+    cs = C.POINTER(C.c_longlong)()
+    nch = C.c_longlong(0)
+    assert lib.chunk_starts(C.byref(plans), C.byref(ft), C.byref(p), total, opts.blocksize,
+                            C.byref(cs), C.byref(nch)) == 0
+    cstarts = np.ctypeslib.as_array(cs, shape=(nch.value,)).copy()
+    C.CDLL(None).free(cs)
+    lib.direct_plans_free(C.byref(plans))
+    return r_lo, lodr, total, cstarts
+
+
+def oracle_metrics(amps: np.ndarray, N: int, dt: float, opts, t_begin: int, count: int,
+                   prec64: bool = False):
+    """Per-trial metrics [nslot, count] from oracle/cs_oracle.c."""
+    lib = oracle_lib()
+    p = opts.params(ref_lib())
+    r_lo, lodr, total, cstarts = ref_chunks(amps, N, dt, opts)
+    decims = np.array(list(p.decimations)[:p.ndecim], dtype=np.int32)
+    nslot = 1 + int((decims > 1).sum())
+    out = np.zeros((nslot, count), dtype=np.float64)
+    a = np.ascontiguousarray(amps, dtype=np.float32)
+    rc = lib.cso_trial_metrics(a.ctypes.data_as(C.POINTER(C.c_float)), a.size // 2, N,
+                               opts.nharms, opts.m, opts.hidr, decims.size,
+                               decims.ctypes.data_as(C.POINTER(C.c_int)), opts.boxcar_fsp,
+                               opts.boxcar_maxfrac, r_lo,
+                               cstarts.ctypes.data_as(C.POINTER(C.c_longlong)), cstarts.size,
+                               total, t_begin, count, int(prec64),
+                               out.ctypes.data_as(C.POINTER(C.c_double)))
+    assert rc == nslot, rc
+    return out, (r_lo, lodr, total, cstarts, decims)
+
+
+def oracle_candidates(metrics: np.ndarray, geo, N: int, dt: float, opts, t_begin: int = 0):
+    """Reference candidate emission (src/search.c:866-905, 705-716) from
+    per-trial metrics: uncollapsed, in (chunk, slot, trial) order."""
+    r_lo, lodr, total, cstarts, decims = geo
+    T = N * dt
+    nyq = N / 2.0
+    ks = [1] + [int(k) for k in decims if k > 1]
+    rows = []
+    count = metrics.shape[1]
+    t = np.arange(t_begin, t_begin + count)
+    chunk = np.searchsorted(cstarts, t, side="right") - 1
+    for c in np.unique(chunk):
+        sel = np.nonzero(chunk == c)[0]
+        i0 = int(cstarts[c])
+        rstart = r_lo + float(i0) * lodr
+        for s, k in enumerate(ks):
+            for i in sel:
+                mval = metrics[s, i]
+                if not (mval > opts.threshold):
+                    continue
+                j = int(t[i]) - i0
+                rf = rstart + float(j) * lodr
+                rsel = float(k) * rf if k != 1 else rf
+                if s and not (rsel < nyq):
+                    continue
+                rows.append((rsel / T, float(mval), rsel, opts.nharms // k, np.nan))
+    return np.array(rows, dtype=nt.CAND_DTYPE)
