@@ -182,6 +182,21 @@ static __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v)
     for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
+/* 16 consecutive accumulator columns of this warp's 32 lanes. */
+static __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
+{
+    uint32_t r[16];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                   "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                   "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
 /* Shared-memory matrix descriptor, canonical K-major layout without swizzle:
  * 8-row x 16-byte core matrices; lbo = byte distance between the two K
  * halves of one MMA (adjacent K core matrices), sbo = between 8-row groups. */
@@ -582,6 +597,8 @@ cs_search_kernel(const SearchArgs args)
     }
 }
 
+#include "cs_search_ws.cuh"
+
 /* ------------------------------------------------------------------ */
 /* Host side                                                          */
 /* ------------------------------------------------------------------ */
@@ -626,6 +643,11 @@ struct GpuSession {
     unsigned *h_count;     /* pinned */
     float last_kernel_ms;
     int own_plans;
+    /* warp-specialised kernel (default ladder at nharms = 60) */
+    int use_ws;
+    float4 *d_Wt;
+    float4 *d_AC;
+    ws60::Harm *d_harm2;
 };
 
 static cudaError_t select_device(int device)
@@ -689,6 +711,9 @@ static void session_release(GpuSession *S)
     cudaFree(S->d_count);
     cudaFree(S->d_err);
     cudaFree(S->d_recs);
+    cudaFree(S->d_Wt);
+    cudaFree(S->d_AC);
+    cudaFree(S->d_harm2);
     if (S->h_count) cudaFreeHost(S->h_count);
     if (S->ev0) cudaEventDestroy(S->ev0);
     if (S->ev1) cudaEventDestroy(S->ev1);
@@ -734,6 +759,39 @@ static int grow_records(GpuSession *S, unsigned cap)
     }
     S->cap = cap;
     return 0;
+}
+
+/* The warp-specialised kernel is compiled for the reference's default
+ * search at nharms = 60: m = 16, decimations 1..6 (all folds), ladder widths
+ * {1,2,3,4,6} for k = 1 and {2,3,4,6} above, and 32-bit trial positions. */
+static int ws60_applies(const CsTables &t, long long total)
+{
+    if (getenv("CS_B200_GENERIC_KERNEL")) return 0;
+    if (t.nh != ws60::NH || t.m != ws60::M || t.nslot != 6) return 0;
+    if (t.kpad != ws60::KPAD || t.npad != ws60::NPAD) return 0;
+    static const int wb[5] = {1, 2, 3, 4, 6}, wd[4] = {2, 3, 4, 6};
+    for (int s = 0; s < 6; s++) {
+        const CsSlot &sl = t.slot[s];
+        if (sl.k != s + 1) return 0;
+        if (s > 0 && !sl.fold) return 0;
+        const int *w = s == 0 ? wb : wd;
+        const int nw = s == 0 ? 5 : 4;
+        if (sl.nw != nw) return 0;
+        for (int i = 0; i < nw; i++) if (sl.widths[i] != w[i]) return 0;
+    }
+    /* 32-bit positions: t < 2^31 and rfloor0 + floor(t*h*pnum/q) + 1 < 2^31 */
+    const double tmax = (double)total + CS_TILE_M;
+    if (tmax >= 2147483647.0) return 0;
+    double rmax = 0;
+    for (int h = 0; h < t.nh; h++) rmax = std::max(rmax, (double)t.harm[h].rfloor0);
+    if (rmax + tmax * t.nh * (double)t.pnum / (double)t.q + 64 >= 2147483647.0) return 0;
+    if ((double)t.q * 5.0 * t.q >= 4294967295.0) return 0;
+    return 1;
+}
+
+static uint32_t magic_for(int d)
+{
+    return d >= 2 ? (uint32_t)(0x100000000ULL / (unsigned long long)d + 1ULL) : 0u;
 }
 
 CS_EXPORT GpuSession *cs_gpu_session_create(const FFTFile *ft, const SearchParams *p,
@@ -815,6 +873,29 @@ CS_EXPORT GpuSession *cs_gpu_session_create(const FFTFile *ft, const SearchParam
     CK(cudaMalloc((void **)&S->d_count, sizeof(unsigned)));
     CK(cudaMalloc((void **)&S->d_err, sizeof(int)));
     CK(cudaMallocHost((void **)&S->h_count, 4 * sizeof(unsigned)));
+    S->use_ws = ws60_applies(S->tab, total) && S->namps < 2147483000LL &&
+                ws60::SMEM_BYTES <= S->max_smem;
+    if (S->use_ws) {
+        std::vector<ws60::Harm> hh(ws60::NH);
+        for (int h = 0; h < ws60::NH; h++) {
+            hh[h].rfloor0 = (int)S->tab.harm[h].rfloor0;
+            hh[h].P = S->tab.harm[h].P;
+            hh[h].woff = S->tab.harm[h].woff;
+            hh[h].wt_off = S->tab.wt_off[h];
+            hh[h].pmagic = magic_for(S->tab.harm[h].P);
+        }
+        CK(cudaMalloc((void **)&S->d_harm2, sizeof(ws60::Harm) * ws60::NH));
+        CK(cudaMemcpy(S->d_harm2, hh.data(), sizeof(ws60::Harm) * ws60::NH,
+                      cudaMemcpyHostToDevice));
+        CK(cudaMalloc((void **)&S->d_Wt, (size_t)S->tab.nrows * S->tab.m * sizeof(float)));
+        CK(cudaMemcpy(S->d_Wt, S->tab.Wt, (size_t)S->tab.nrows * S->tab.m * sizeof(float),
+                      cudaMemcpyHostToDevice));
+        CK(cudaMalloc((void **)&S->d_AC, (size_t)S->tab.nrows * 4 * sizeof(float)));
+        CK(cudaMemcpy(S->d_AC, S->tab.AC, (size_t)S->tab.nrows * 4 * sizeof(float),
+                      cudaMemcpyHostToDevice));
+        CK(cudaFuncSetAttribute(ws60::search_ws60, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                ws60::SMEM_BYTES));
+    }
     {
         /* Start with room for 1 in 16 trials per slot; grown on overflow. */
         long long want = (total * S->tab.nslot) / 16 + 4096;
@@ -889,6 +970,34 @@ static cudaError_t enqueue_search(GpuSession *S, const float2 *d_amps, double th
         cs_amax_kernel<<<g, 256, 0, S->st>>>(d_amps, S->namps, S->d_amax);
     }
     if (S->tab.ntiles <= 0) return cudaGetLastError();
+    if (S->use_ws) {
+        ws60::Args w;
+        memset(&w, 0, sizeof(w));
+        w.amps = d_amps;
+        w.namps = (int)S->namps;
+        w.Wt = S->d_Wt;
+        w.AC = S->d_AC;
+        w.harm = S->d_harm2;
+        w.chunks = S->d_chunks;
+        w.tiles = S->d_tiles;
+        w.ntiles = S->tab.ntiles;
+        w.bimg = S->d_bimg;
+        w.q = S->tab.q;
+        w.pnum = S->tab.pnum;
+        w.qmagic = magic_for(S->tab.q);
+        w.gbound = S->tab.gbound;
+        w.amax = S->d_amax;
+        w.thresh = threshold;
+        w.recs = S->d_recs;
+        w.count = S->d_count;
+        w.cap = S->cap;
+        w.err = S->d_err;
+        const int grid = std::min(S->tab.ntiles, S->nsm);
+        if (timed) cudaEventRecord(S->ev0, S->st);
+        ws60::search_ws60<<<grid, ws60::NTHREADS, ws60::SMEM_BYTES, S->st>>>(w);
+        if (timed) cudaEventRecord(S->ev1, S->st);
+        return cudaGetLastError();
+    }
     const SearchArgs a = make_args(S, d_amps, threshold);
     const int smem = smem_bytes(S->tab);
     const int grid = std::min(S->tab.ntiles, S->nsm);
@@ -1010,8 +1119,9 @@ CS_EXPORT int cs_b200_session_info(const GpuSession *S, CsB200Info *info)
     info->nslot = S->tab.nslot;
     info->npad = S->tab.npad;
     info->kpad = S->tab.kpad;
-    info->smem_bytes = smem_bytes(S->tab);
+    info->smem_bytes = S->use_ws ? ws60::SMEM_BYTES : smem_bytes(S->tab);
     info->grid = std::min(S->tab.ntiles, S->nsm);
+    info->kernel = S->use_ws ? 1 : 0;
     info->total = S->total;
     info->rec_capacity = S->cap;
     return 0;

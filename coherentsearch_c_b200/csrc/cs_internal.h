@@ -74,6 +74,13 @@ typedef struct {
     uint8_t *carry;            /* nrows */
     uint16_t *rowtab;          /* nh * q: residue -> phase index */
     float gbound;              /* max over rows of (|A_re|+|A_im|) * sum|W| */
+    /* layout for the warp-specialised kernel (m % 4 == 0):
+     *   Wt: per harmonic, [m/4][P] float4 -- lanes on consecutive phases
+     *       read consecutive 16-byte words;
+     *   AC: per row float4 {A_re, A_im, carry (int bits), 0} */
+    float *Wt;                 /* nrows * m */
+    float *AC;                 /* nrows * 4 */
+    int wt_off[CS_MAX_NH];     /* first float4 of harmonic h in Wt */
 } CsTables;
 
 /* Build / free the tables.  Returns 0 or -1 with a message in err. */

@@ -1,0 +1,469 @@
+/*
+ * Warp-specialised search kernel for the default decimation ladder
+ * (nharms = 60, m = 16, k = 1..6, ladder widths {1,2,3,4,6} / {2,3,4,6}).
+ *
+ * One persistent CTA per SM, 16 warps:
+ *   warps 0-7   interpolation: tile i -> fp16 hi/lo A operand in shared
+ *               memory buffer i%2 (same FP32 arithmetic as the generic
+ *               kernel, bit-identical harmonic amplitudes);
+ *   warps 8-15  tensor-core issue (one elected thread) and the boxcar
+ *               epilogue of tile i from tensor-memory accumulator i%2 while
+ *               the interpolation warps fill the other A buffer.
+ * Hand-off through mbarriers: a_full (8 warp arrivals), a_empty and d_full
+ * (tcgen05.commit).  The epilogue keeps every prefix sum in registers: with
+ * the bin count and widths known at compile time, the cyclic prefix, the
+ * sliding window differences P[i] - P[i-w] and the k-fold sums all unroll
+ * into straight-line FP32 code in the reference's expression order.
+ */
+#pragma once
+
+namespace ws60 {
+
+constexpr int NH = 60;
+constexpr int NB = 2 * NH;          /* 120 bins */
+constexpr int M = 16;               /* interpolation taps */
+constexpr int NTHREADS = 512;
+constexpr int KPAD = 128;
+constexpr int NPAD = 128;
+constexpr int AIMG = CS_TILE_M * KPAD * 2;   /* one fp16 A image */
+constexpr int BIMG = NPAD * KPAD * 2;        /* one fp16 B image */
+constexpr int TMEM_COLS = 256;               /* two 128-column accumulators */
+
+/* ladder widths: {1,2,3,4,6} at k = 1, {2,3,4,6} above (src/boxcar.c:100-133) */
+struct WBase {
+    static constexpr int n = 5, wmax = 6;
+    static __host__ __device__ constexpr int w(int a) { return a < 4 ? a + 1 : 6; }
+};
+struct WDec {
+    static constexpr int n = 4, wmax = 6;
+    static __host__ __device__ constexpr int w(int a) { return a < 3 ? a + 2 : 6; }
+};
+
+/* per-harmonic header in shared memory */
+struct Harm {
+    int rfloor0;
+    int P;
+    int woff;        /* row of phase 0 in AC */
+    int wt_off;      /* float4 index of (tap quad 0, phase 0) in Wt */
+    uint32_t pmagic; /* floor(2^32 / P) + 1, or 0 for P == 1 */
+};
+
+struct Args {
+    const float2 *amps;
+    int namps;
+    const float4 *Wt;
+    const float4 *AC;
+    const Harm *harm;
+    const CsChunk *chunks;
+    const int *tiles;
+    int ntiles;
+    const uint4 *bimg;
+    int q, pnum;
+    uint32_t qmagic;
+    float gbound;
+    const unsigned *amax;
+    double thresh;
+    CsRec *recs;
+    unsigned *count;
+    unsigned cap;
+    int *err;
+};
+
+/* shared memory: B hi/lo | A0 hi/lo | A1 hi/lo | barriers | tmem slot */
+constexpr int SM_B = 0;
+constexpr int SM_A = 2 * BIMG;
+constexpr int SM_BAR = SM_A + 4 * AIMG;
+constexpr int SM_TM = SM_BAR + 64;
+constexpr int SM_HARM = SM_TM + 16;
+constexpr int SMEM_BYTES = SM_HARM + NH * (int)sizeof(Harm);
+
+template <class WS>
+struct Scan {
+    float hist[WS::wmax + 1];   /* hist[j] = P[i - j] */
+    float mx[WS::n];
+    float P, tot;
+};
+
+template <class WS>
+static __device__ __forceinline__ void scan_init(Scan<WS> &s)
+{
+    s.P = 0.0f;
+    s.tot = 0.0f;
+#pragma unroll
+    for (int j = 0; j <= WS::wmax; j++) s.hist[j] = 0.0f;
+#pragma unroll
+    for (int a = 0; a < WS::n; a++) s.mx[a] = -INFINITY;
+}
+
+/* Append profile element x as the i-th step (i = 1 .. NK + wmax) of the
+ * cyclic prefix sum: P[i] = P[i-1] + x, then every window of width w ending
+ * at i (start position p = i - w + 1 in 1..NK) contributes P[i] - P[i-w]
+ * (src/boxcar.c:207-226).  i is a compile-time constant after unrolling. */
+template <int NK, class WS>
+static __device__ __forceinline__ void scan_push(Scan<WS> &s, float x, int i)
+{
+    s.P = __fadd_rn(s.P, x);
+#pragma unroll
+    for (int j = WS::wmax; j > 0; j--) s.hist[j] = s.hist[j - 1];
+    s.hist[0] = s.P;
+    if (i == NK) s.tot = s.P;
+#pragma unroll
+    for (int a = 0; a < WS::n; a++) {
+        const int w = WS::w(a);
+        const int p = i - w + 1;
+        if (p >= 1 && p <= NK) s.mx[a] = fmaxf(s.mx[a], __fsub_rn(s.hist[0], s.hist[w]));
+    }
+}
+
+/* max_w (M_w - duty_w * total) * invsw_w with duty_w = (float)w / (float)NK
+ * (src/boxcar.c:220-228; a compile-time constant here). */
+template <int NK, class WS>
+static __device__ __forceinline__ float scan_finish(const Scan<WS> &s, const float *invsw)
+{
+    float best = -INFINITY;
+#pragma unroll
+    for (int a = 0; a < WS::n; a++) {
+        const float duty = (float)WS::w(a) / (float)NK;
+        best = fmaxf(best, __fmul_rn(__fsub_rn(s.mx[a], __fmul_rn(duty, s.tot)), invsw[a]));
+    }
+    return best;
+}
+
+/* Full-resolution profile: columns 0..NB-1 of the accumulator row. */
+static __device__ __forceinline__ float base_metric(uint32_t trow, const float *invsw)
+{
+    Scan<WBase> s;
+    scan_init(s);
+    float first[WBase::wmax];
+#pragma unroll
+    for (int c = 0; c < (NB + 31) / 32; c++) {
+        float v[32];
+        tmem_ld32(trow + 32 * c, v);
+#pragma unroll
+        for (int u = 0; u < 32; u++) {
+            const int i = 32 * c + u + 1;
+            if (i <= NB) {
+                if (i - 1 < WBase::wmax) first[i - 1] = v[u];
+                scan_push<NB, WBase>(s, v[u], i);
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < WBase::wmax; u++) scan_push<NB, WBase>(s, first[u], NB + 1 + u);
+    return scan_finish<NB>(s, invsw);
+}
+
+/* k-fold average of the full profile (src/search.c:298-331): r[j] is the
+ * left-to-right FP32 sum of x[j + q*NK], times (1/k), then the boxcar. */
+template <int K>
+static __device__ __forceinline__ float fold_metric(uint32_t trow, const float *invsw)
+{
+    constexpr int NK = NB / K;
+    float r[NK];
+#pragma unroll
+    for (int c = 0; c < (NB + 15) / 16; c++) {
+        float v[16];
+        tmem_ld16(trow + 16 * c, v);
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            const int i = 16 * c + u;
+            if (i < NB) {
+                if (i < NK) r[i % NK] = v[u];
+                else r[i % NK] = __fadd_rn(r[i % NK], v[u]);
+            }
+        }
+    }
+    const float invk = 1.0f / (float)K;
+    Scan<WDec> s;
+    scan_init(s);
+#pragma unroll
+    for (int j = 0; j < NK; j++) {
+        r[j] = __fmul_rn(r[j], invk);
+        scan_push<NK, WDec>(s, r[j], j + 1);
+    }
+#pragma unroll
+    for (int u = 0; u < WDec::wmax; u++) scan_push<NK, WDec>(s, r[u], NK + 1 + u);
+    return scan_finish<NK>(s, invsw);
+}
+
+static __device__ __forceinline__ void emit(const Args &a, bool hit, int ci, int slot, int j,
+                                            float metric, int lane)
+{
+    const unsigned mask = __ballot_sync(0xffffffffu, hit);
+    if (!mask) return;
+    unsigned basei = 0;
+    if (lane == 0) basei = atomicAdd(a.count, (unsigned)__popc(mask));
+    basei = __shfl_sync(0xffffffffu, basei, 0);
+    if (hit) {
+        const unsigned pos = basei + (unsigned)__popc(mask & ((1u << lane) - 1u));
+        if (pos < a.cap) {
+            CsRec rec;
+            rec.chunk = ci;
+            rec.slot = slot;
+            rec.j = j;
+            rec.metric = metric;
+            a.recs[pos] = rec;
+        }
+    }
+}
+
+static __device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(bar) : "memory");
+}
+
+/* barrier over the 256 epilogue threads with an AND vote */
+static __device__ __forceinline__ bool epi_bar_and(bool v)
+{
+    uint32_t out;
+    asm volatile("{\n\t.reg .pred p, q;\n\t"
+                 "setp.ne.u32 p, %1, 0;\n\t"
+                 "bar.red.and.pred q, 1, 256, p;\n\t"
+                 "selp.u32 %0, 1, 0, q;\n\t}"
+                 : "=r"(out) : "r"((uint32_t)v) : "memory");
+    return out != 0;
+}
+
+static __device__ __forceinline__ uint32_t mod_magic(uint32_t t, uint32_t P, uint32_t magic)
+{
+    if (P == 1) return 0;
+    uint32_t e = __umulhi(t, magic);
+    uint32_t pr = e * P;
+    if (pr > t) pr -= P;
+    return t - pr;
+}
+
+__global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const Args a)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t bar_afull = smem_u32(smem + SM_BAR);        /* 2 x 8 B */
+    const uint32_t bar_aempty = bar_afull + 16;
+    const uint32_t bar_dfull = bar_afull + 32;
+    uint32_t *tm_slot = reinterpret_cast<uint32_t *>(smem + SM_TM);
+    Harm *hs = reinterpret_cast<Harm *>(smem + SM_HARM);
+
+    if (warp == 0) tmem_alloc(smem_u32(tm_slot), TMEM_COLS);
+    if (tid == 0) {
+        mbar_init(bar_afull, 8);
+        mbar_init(bar_afull + 8, 8);
+        mbar_init(bar_aempty, 1);
+        mbar_init(bar_aempty + 8, 1);
+        mbar_init(bar_dfull, 1);
+        mbar_init(bar_dfull + 8, 1);
+    }
+    for (int h = tid; h < NH; h += NTHREADS) hs[h] = a.harm[h];
+    {
+        uint4 *dst = reinterpret_cast<uint4 *>(smem + SM_B);
+        for (int i = tid; i < (2 * BIMG) / 16; i += NTHREADS) dst[i] = a.bimg[i];
+        /* the K padding block (k = 120..127) of both A buffers stays zero */
+        for (int i = tid; i < 4 * CS_TILE_M; i += NTHREADS) {
+            const int img = i / CS_TILE_M, r = i % CS_TILE_M;
+            const uint32_t off = (uint32_t)img * AIMG + 15u * (CS_TILE_M * 16) +
+                                 (uint32_t)(r >> 3) * 128 + (uint32_t)(r & 7) * 16;
+            *reinterpret_cast<uint4 *>(smem + SM_A + off) = make_uint4(0, 0, 0, 0);
+        }
+    }
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tm_slot;
+    const float scale = operand_scale(a.amax, a.gbound);
+    const float inv_scale = 1.0f / scale;
+
+    if (warp < 8) {
+        /* ------------------------- interpolation ------------------------- */
+        const int r = tid & (CS_TILE_M - 1);
+        const int par = tid >> 7;
+        int it = 0;
+        for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, it++) {
+            const int s = it & 1;
+            if (it >= 2 && !mbar_wait(bar_aempty + 8 * s, ((it - 2) >> 1) & 1)) {
+                if (lane == 0) atomicExch(a.err, 1);
+                break;
+            }
+            const int ci = a.tiles[3 * tile], j0 = a.tiles[3 * tile + 1];
+            const int cnt = a.tiles[3 * tile + 2];
+            const CsChunk &ch = a.chunks[ci];
+            const unsigned long long filled = ch.filled;
+            const bool valid = r < cnt;
+            const uint32_t t = (uint32_t)(ch.i0 + j0 + r);
+            uint32_t Q, R;
+            if (a.pnum == 1) {
+                divmod_q(t, (uint32_t)a.q, a.qmagic, Q, R);
+            } else {
+                const unsigned long long tp = (unsigned long long)t * (unsigned)a.pnum;
+                Q = (uint32_t)(tp / (unsigned)a.q);
+                R = (uint32_t)(tp - (unsigned long long)Q * (unsigned)a.q);
+            }
+            /* residue/quotient of t*h*pnum for h = 4*par+1, and the steps +1, +5 */
+            uint32_t res, qint, q5, r5;
+            {
+                const uint32_t h0 = 4u * par + 1u;
+                uint32_t qd;
+                divmod_q(h0 * R, (uint32_t)a.q, a.qmagic, qd, res);
+                qint = h0 * Q + qd;
+                divmod_q(5u * R, (uint32_t)a.q, a.qmagic, qd, r5);
+                q5 = 5u * Q + qd;
+            }
+            unsigned char *abuf = smem + SM_A + s * 2 * AIMG;
+            for (int hb = par; hb < NH / 4; hb += 2) {
+                uint32_t hw[4], lw[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int h = 4 * hb + u + 1;
+                    float xr = 0.0f, xi = 0.0f;
+                    if (valid && ((filled >> (h - 1)) & 1ULL)) {
+                        const Harm hm = hs[h - 1];
+                        const uint32_t ph = mod_magic(t, (uint32_t)hm.P, hm.pmagic);
+                        const float4 ac = __ldg(a.AC + hm.woff + ph);
+                        const int base = hm.rfloor0 + (int)qint + __float_as_int(ac.z);
+                        const int b0 = base + 1 - M / 2;
+                        float ar = 0.0f, ai = 0.0f;
+                        if ((unsigned)b0 <= (unsigned)(a.namps - M)) {
+                            const float2 *ap = a.amps + b0;
+                            const float4 *wq = a.Wt + hm.wt_off + ph;
+#pragma unroll
+                            for (int i4 = 0; i4 < M / 4; i4++) {
+                                const float4 w = __ldg(wq + i4 * hm.P);
+                                const float2 v0 = __ldg(ap + 4 * i4), v1 = __ldg(ap + 4 * i4 + 1);
+                                const float2 v2 = __ldg(ap + 4 * i4 + 2), v3 = __ldg(ap + 4 * i4 + 3);
+                                ar = __fmaf_rn(w.x, v0.x, ar); ai = __fmaf_rn(w.x, v0.y, ai);
+                                ar = __fmaf_rn(w.y, v1.x, ar); ai = __fmaf_rn(w.y, v1.y, ai);
+                                ar = __fmaf_rn(w.z, v2.x, ar); ai = __fmaf_rn(w.z, v2.y, ai);
+                                ar = __fmaf_rn(w.w, v3.x, ar); ai = __fmaf_rn(w.w, v3.y, ai);
+                            }
+                        }
+                        xr = __fsub_rn(__fmul_rn(ac.x, ar), __fmul_rn(ac.y, ai));
+                        xi = __fadd_rn(__fmul_rn(ac.x, ai), __fmul_rn(ac.y, ar));
+                    }
+                    const float2 sc = make_float2(xr * scale, xi * scale);
+                    const __half2 hi = __float22half2_rn(sc);
+                    const float2 back = __half22float2(hi);
+                    const __half2 lo = __float22half2_rn(
+                        make_float2(__fsub_rn(sc.x, back.x), __fsub_rn(sc.y, back.y)));
+                    hw[u] = *reinterpret_cast<const uint32_t *>(&hi);
+                    lw[u] = *reinterpret_cast<const uint32_t *>(&lo);
+                    if (u < 3) {           /* advance h -> h+1 */
+                        res += R; qint += Q;
+                        if (res >= (uint32_t)a.q) { res -= (uint32_t)a.q; qint += 1; }
+                    }
+                }
+                /* h -> h+5: from 4hb+4 to the first harmonic of block hb+2 */
+                res += r5; qint += q5;
+                if (res >= (uint32_t)a.q) { res -= (uint32_t)a.q; qint += 1; }
+                const uint32_t off = (uint32_t)hb * (CS_TILE_M * 16) + (uint32_t)(r >> 3) * 128 +
+                                     (uint32_t)(r & 7) * 16;
+                *reinterpret_cast<uint4 *>(abuf + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                *reinterpret_cast<uint4 *>(abuf + AIMG + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+            }
+            fence_proxy_async();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar_afull + 8 * s);
+        }
+    } else {
+        /* --------------------- tensor cores + epilogue --------------------- */
+        const int e = warp - 8;
+        const int quarter = e & 3, grp = e >> 2;
+        const int r = quarter * 32 + lane;
+        const bool leader = (warp == 8 && lane == 0);
+        const uint32_t idesc = (1u << 4) | ((uint32_t)(NPAD >> 3) << 17) |
+                               ((uint32_t)(CS_TILE_M >> 4) << 24);
+        const uint32_t lbo_a = CS_TILE_M * 16, lbo_b = NPAD * 16;
+        const uint32_t b_hi = smem_u32(smem + SM_B), b_lo = b_hi + BIMG;
+        int issued = 0, consumed = 0;
+        bool ok = true;
+
+        auto issue = [&](int it) -> bool {
+            const int s = it & 1;
+            if (!mbar_wait(bar_afull + 8 * s, (it >> 1) & 1)) return false;
+            tc_fence_after();
+            const uint32_t a_hi = smem_u32(smem + SM_A + s * 2 * AIMG), a_lo = a_hi + AIMG;
+            const uint32_t d = tmem + (uint32_t)(s * 128);
+            uint32_t acc = 0;
+#pragma unroll
+            for (int pass = 0; pass < 3; pass++) {
+                const uint32_t abase = (pass == 1) ? a_lo : a_hi;
+                const uint32_t bbase = (pass == 2) ? b_lo : b_hi;
+#pragma unroll
+                for (int k = 0; k < KPAD / 16; k++) {
+                    mma_f16(d, umma_desc(abase + (uint32_t)k * 2 * lbo_a, lbo_a, 128),
+                            umma_desc(bbase + (uint32_t)k * 2 * lbo_b, lbo_b, 128), idesc, acc);
+                    acc = 1;
+                }
+            }
+            mma_commit(bar_aempty + 8 * s);
+            mma_commit(bar_dfull + 8 * s);
+            return true;
+        };
+
+        if (leader && (int)blockIdx.x < a.ntiles) {
+            ok = issue(0);
+            if (ok) issued = 1;
+            else atomicExch(a.err, 1);
+        }
+        int it = 0;
+        for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, it++) {
+            const int s = it & 1;
+            if (leader && ok && tile + (int)gridDim.x < a.ntiles) {
+                ok = issue(it + 1);
+                if (ok) issued++;
+                else atomicExch(a.err, 1);
+            }
+            bool got = mbar_wait(bar_dfull + 8 * s, (it >> 1) & 1);
+            if (!epi_bar_and(got && ok)) {
+                if (lane == 0) atomicExch(a.err, 1);
+                ok = false;
+                break;
+            }
+            consumed++;
+            tc_fence_after();
+            const int ci = a.tiles[3 * tile], j0 = a.tiles[3 * tile + 1];
+            const int cnt = a.tiles[3 * tile + 2];
+            const CsChunk &ch = a.chunks[ci];
+            const bool valid = r < cnt;
+            const int j = j0 + r;
+            const uint32_t trow = tmem + (uint32_t)(s * 128) + ((uint32_t)(quarter * 32) << 16);
+            if (grp == 0) {
+                float iv[5], iw[4];
+#pragma unroll
+                for (int q = 0; q < 5; q++) iv[q] = ch.invsw[0][q];
+#pragma unroll
+                for (int q = 0; q < 4; q++) iw[q] = ch.invsw[5][q];
+                const float m0 = base_metric(trow, iv) * inv_scale;
+                const float m5 = fold_metric<6>(trow, iw) * inv_scale;
+                emit(a, valid && j < ch.nvalid[0] && (double)m0 > a.thresh, ci, 0, j, m0, lane);
+                emit(a, valid && j < ch.nvalid[5] && (double)m5 > a.thresh, ci, 5, j, m5, lane);
+            } else {
+                float iw[4][4];
+#pragma unroll
+                for (int sl = 0; sl < 4; sl++)
+#pragma unroll
+                    for (int q = 0; q < 4; q++) iw[sl][q] = ch.invsw[sl + 1][q];
+                const float m1 = fold_metric<2>(trow, iw[0]) * inv_scale;
+                emit(a, valid && j < ch.nvalid[1] && (double)m1 > a.thresh, ci, 1, j, m1, lane);
+                const float m2 = fold_metric<3>(trow, iw[1]) * inv_scale;
+                emit(a, valid && j < ch.nvalid[2] && (double)m2 > a.thresh, ci, 2, j, m2, lane);
+                const float m3 = fold_metric<4>(trow, iw[2]) * inv_scale;
+                emit(a, valid && j < ch.nvalid[3] && (double)m3 > a.thresh, ci, 3, j, m3, lane);
+                const float m4 = fold_metric<5>(trow, iw[3]) * inv_scale;
+                emit(a, valid && j < ch.nvalid[4] && (double)m4 > a.thresh, ci, 4, j, m4, lane);
+            }
+            tc_fence_before();
+            epi_bar_and(true);      /* accumulator s free for the MMA of tile it+2 */
+        }
+        /* drain: never free tensor memory under an MMA in flight */
+        if (leader) {
+            for (int k = consumed; k < issued; k++)
+                mbar_wait(bar_dfull + 8 * (k & 1), (k >> 1) & 1);
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, TMEM_COLS);
+    }
+}
+
+}  // namespace ws60

@@ -68,6 +68,8 @@ CS_HIDDEN_API void cs_tables_free(CsTables *t)
     free(t->A);
     free(t->carry);
     free(t->rowtab);
+    free(t->Wt);
+    free(t->AC);
     memset(t, 0, sizeof(*t));
 }
 
@@ -265,6 +267,40 @@ CS_HIDDEN_API int cs_tables_build(CsTables *t, const FFTFile *ft, const SearchPa
     }
     /* pad the bound by 1% for the FP32 rounding of the accumulation */
     t->gbound = (float)(gmax * 1.01 + 1e-30);
+
+    /* transposed weights and packed phase factor + carry */
+    t->Wt = (float *)malloc((size_t)nrows * t->m * sizeof(float));
+    t->AC = (float *)malloc((size_t)nrows * 4 * sizeof(float));
+    if (!t->Wt || !t->AC) {
+        snprintf(err, errlen, "out of host memory");
+        return -1;
+    }
+    {
+        int f4 = 0;
+        const int m4 = (t->m + 3) / 4;
+        for (h = 1; h <= nh; h++) {
+            const int P = t->harm[h - 1].P, off = t->harm[h - 1].woff;
+            t->wt_off[h - 1] = f4;
+            int ph, i4, e;
+            for (i4 = 0; i4 < m4; i4++)
+                for (ph = 0; ph < P; ph++)
+                    for (e = 0; e < 4; e++) {
+                        const int tap = 4 * i4 + e;
+                        t->Wt[4 * (size_t)(f4 + i4 * P + ph) + e] =
+                            tap < t->m ? t->W[(size_t)(off + ph) * t->m + tap] : 0.0f;
+                    }
+            for (ph = 0; ph < P; ph++) {
+                int32_t cbits = t->carry[off + ph];
+                float cf;
+                memcpy(&cf, &cbits, sizeof(cf));
+                t->AC[4 * (off + ph) + 0] = t->A[2 * (off + ph) + 0];
+                t->AC[4 * (off + ph) + 1] = t->A[2 * (off + ph) + 1];
+                t->AC[4 * (off + ph) + 2] = cf;
+                t->AC[4 * (off + ph) + 3] = 0.0f;
+            }
+            f4 += m4 * P;
+        }
+    }
     return 0;
 }
 

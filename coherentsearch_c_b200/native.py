@@ -68,7 +68,8 @@ class DirectPlanSet(C.Structure):
 class CsB200Info(C.Structure):
     _fields_ = [("ntiles", C.c_int), ("nchunks", C.c_longlong), ("nslot", C.c_int),
                 ("npad", C.c_int), ("kpad", C.c_int), ("smem_bytes", C.c_int),
-                ("grid", C.c_int), ("total", C.c_longlong), ("rec_capacity", C.c_uint)]
+                ("grid", C.c_int), ("total", C.c_longlong), ("rec_capacity", C.c_uint),
+                ("kernel", C.c_int)]
 
 
 CAND_DTYPE = np.dtype([("freq", "f8"), ("metric", "f8"), ("r", "f8"), ("nharm", "i4"),

@@ -27,6 +27,8 @@ typedef struct {
     int grid;            /* persistent CTAs launched */
     long long total;     /* trials */
     unsigned rec_capacity;
+    int kernel;          /* 0: generic fused kernel, 1: warp-specialised
+                            kernel for the default nharms = 60 ladder */
 } CsB200Info;
 
 int cs_b200_session_info(const GpuSession *s, CsB200Info *info);

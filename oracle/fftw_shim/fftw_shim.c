@@ -210,6 +210,72 @@ static eng_##S *eng_new_##S(int n, int sign)                                    
 DEFINE_ENGINE(float, f)
 DEFINE_ENGINE(double, d)
 
+
+/* ------------------------------------------------------------------ */
+/* Batch-vectorised engine: 16 independent float transforms per vector */
+/* (the batch index is contiguous in the reference's c2r plans,        */
+/* src/search.c:180-187: istride = Nprof, idist = 1).                  */
+/* ------------------------------------------------------------------ */
+typedef float v16 __attribute__((vector_size(64)));
+typedef struct { v16 re, im; } cxv;
+
+static void recv(const eng_f *e, int n, int tws, const cxv *in, long is, cxv *out, int depth)
+{
+    if (n == 1) { out[0] = in[0]; return; }
+    const int p = e->fac[depth];
+    const int m = n / p;
+    int r, k;
+    for (r = 0; r < p; r++)
+        recv(e, m, tws * p, in + (long)r * is, is * p, out + (long)r * m, depth + 1);
+    const int N = e->n;
+    const cx_f *tw = e->tw;
+    for (k = 0; k < m; k++) {
+        cxv t[64];
+        t[0] = out[k];
+        for (r = 1; r < p; r++) {
+            const cxv a = out[(long)r * m + k];
+            const cx_f w = tw[(long)r * k * tws];
+            t[r].re = a.re * w.re - a.im * w.im;
+            t[r].im = a.re * w.im + a.im * w.re;
+        }
+        if (p == 2) {
+            out[k].re = t[0].re + t[1].re; out[k].im = t[0].im + t[1].im;
+            out[m + k].re = t[0].re - t[1].re; out[m + k].im = t[0].im - t[1].im;
+        } else if (p == 4) {
+            const float s = (float)e->sign;
+            const v16 a0r = t[0].re + t[2].re, a0i = t[0].im + t[2].im;
+            const v16 a1r = t[0].re - t[2].re, a1i = t[0].im - t[2].im;
+            const v16 b0r = t[1].re + t[3].re, b0i = t[1].im + t[3].im;
+            const v16 b1r = t[1].re - t[3].re, b1i = t[1].im - t[3].im;
+            out[k].re = a0r + b0r; out[k].im = a0i + b0i;
+            out[2 * m + k].re = a0r - b0r; out[2 * m + k].im = a0i - b0i;
+            out[m + k].re = a1r - s * b1i; out[m + k].im = a1i + s * b1r;
+            out[3 * m + k].re = a1r + s * b1i; out[3 * m + k].im = a1i - s * b1r;
+        } else if (p == 3) {
+            const float c3 = (float)(0.86602540378443864676372317075293618 * e->sign);
+            const v16 ar = t[1].re + t[2].re, ai = t[1].im + t[2].im;
+            const v16 br = t[1].re - t[2].re, bi = t[1].im - t[2].im;
+            const v16 mr = t[0].re - 0.5f * ar, mi = t[0].im - 0.5f * ai;
+            out[k].re = t[0].re + ar; out[k].im = t[0].im + ai;
+            out[m + k].re = mr - c3 * bi; out[m + k].im = mi + c3 * br;
+            out[2 * m + k].re = mr + c3 * bi; out[2 * m + k].im = mi - c3 * br;
+        } else {
+            int q;
+            for (q = 0; q < p; q++) {
+                v16 sr = t[0].re, si = t[0].im;
+                for (r = 1; r < p; r++) {
+                    const long idx = ((long)r * q % p) * (long)m * tws;
+                    const cx_f w = tw[idx % N];
+                    sr += t[r].re * w.re - t[r].im * w.im;
+                    si += t[r].re * w.im + t[r].im * w.re;
+                }
+                out[(long)q * m + k].re = sr;
+                out[(long)q * m + k].im = si;
+            }
+        }
+    }
+}
+
 /* ------------------------------------------------------------------ */
 /* Plans                                                               */
 /* ------------------------------------------------------------------ */
@@ -311,6 +377,55 @@ fftwf_plan fftwf_plan_dft_1d(int n, fftwf_complex *in, fftwf_complex *out,
     return p;
 }
 
+
+/* Float c2r of 16 transforms at a time through the vector engine; returns
+ * how many transforms it handled (a multiple of 16, or 0). */
+static int c2r_batch16_f(struct cs_shim_plan *p)
+{
+    const int n = p->n, N = n / 2;
+    if (p->idist != 1 || p->howmany < 16 || p->ef->blue || N > 256 || N < 1) return 0;
+    const float *in = (const float *)p->in;
+    float *out = (float *)p->out;
+    const cx_f *tw = (const cx_f *)p->tw_half;
+    cxv Z[256], z[256];
+    int b0, k, j, l;
+    const int nb = p->howmany / 16 * 16;
+    for (b0 = 0; b0 < nb; b0 += 16) {
+        for (k = 0; k < N; k++) {
+            const float *xa = in + 2 * ((long)k * p->istride + b0);
+            const float *xb = in + 2 * ((long)(N - k) * p->istride + b0);
+            float g[4][16];
+            for (l = 0; l < 16; l++) {
+                g[0][l] = xa[2 * l];
+                g[1][l] = k ? xa[2 * l + 1] : 0.0f;
+                g[2][l] = xb[2 * l];
+                g[3][l] = k ? -xb[2 * l + 1] : 0.0f;
+            }
+            v16 ar, ai, br, bi;
+            memcpy(&ar, g[0], sizeof(ar));
+            memcpy(&ai, g[1], sizeof(ai));
+            memcpy(&br, g[2], sizeof(br));
+            memcpy(&bi, g[3], sizeof(bi));
+            const v16 er = ar + br, ei = ai + bi;
+            const v16 dr = ar - br, di = ai - bi;
+            const v16 orr = dr * tw[k].re - di * tw[k].im;
+            const v16 oi = dr * tw[k].im + di * tw[k].re;
+            Z[k].re = er - oi;
+            Z[k].im = ei + orr;
+        }
+        recv(p->ef, N, 1, Z, 1, z, 0);
+        for (l = 0; l < 16; l++) {
+            float *y = out + (long)(b0 + l) * p->odist;
+            for (j = 0; j < N; j++) {
+                y[(long)(2 * j) * p->ostride] = z[j].re[l];
+                y[(long)(2 * j + 1) * p->ostride] = z[j].im[l];
+            }
+        }
+    }
+    return nb;
+}
+static int c2r_batch16_d(struct cs_shim_plan *p) { (void)p; return 0; }
+
 /* Even-length c2r through one complex FFT of length n/2:
  *   E[k] = X[k] + conj(X[N-k]),  O[k] = (X[k] - conj(X[N-k])) exp(2 pi i k/n)
  *   z = backward DFT_N(E + i O);  y[2j] = Re z[j], y[2j+1] = Im z[j]. */
@@ -342,7 +457,8 @@ static void c2r_exec_##S(struct cs_shim_plan *p)                                
     const int N = n / 2;                                                         \
     cx_##S *Z = (cx_##S *)p->zbuf, *z = Z + N;                                   \
     const cx_##S *tw = (const cx_##S *)p->tw_half;                               \
-    for (b = 0; b < p->howmany; b++) {                                           \
+    b = c2r_batch16_##S(p);                                                      \
+    for (; b < p->howmany; b++) {                                                \
         const R *x = in + 2 * (long)b * p->idist;                                \
         int k;                                                                   \
         for (k = 0; k < N; k++) {                                                \

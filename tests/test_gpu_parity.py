@@ -43,11 +43,19 @@ def match_candidates(a, b, thr, rtol):
     return only_a, only_b
 
 
-def test_all_trial_metrics_vs_oracle(gpu_ready):
+@pytest.mark.parametrize("nharms,kernel", [(60, "ws"), (60, "generic"), (32, "generic"),
+                                           (16, "generic"), (7, "generic")])
+def test_all_trial_metrics_vs_oracle(gpu_ready, monkeypatch, nharms, kernel):
     """Every trial of every decimation slot: GPU metric vs the oracle's."""
+    if kernel == "generic":
+        monkeypatch.setenv("CS_B200_GENERIC_KERNEL", "1")
+    else:
+        monkeypatch.delenv("CS_B200_GENERIC_KERNEL", raising=False)
     spec, amps = _small_case()
-    opts = Options(blocksize=2048, threshold=-1e30, remove=False, harm_remove=False)
+    opts = Options(nharms=nharms, blocksize=2048, threshold=-1e30, remove=False,
+                   harm_remove=False)
     ses = Session(spec.N, spec.dt, opts)
+    assert ses.info().kernel == (1 if kernel == "ws" else 0)
     raw = ses.run_raw(amps)
     total = ses.total
     met, geo = rb.oracle_metrics(amps, spec.N, spec.dt, opts, 0, total)
