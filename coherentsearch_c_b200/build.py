@@ -57,7 +57,7 @@ def _newer(out, deps):
 
 def _headers():
     hs = [os.path.join(INC, f) for f in os.listdir(INC) if f.endswith(".h")]
-    hs += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
+    hs += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     return hs
 
 

@@ -883,6 +883,7 @@ CS_EXPORT GpuSession *cs_gpu_session_create(const FFTFile *ft, const SearchParam
             hh[h].woff = S->tab.harm[h].woff;
             hh[h].wt_off = S->tab.wt_off[h];
             hh[h].pmagic = magic_for(S->tab.harm[h].P);
+            hh[h].carry_res = S->tab.carry_res[h];
         }
         CK(cudaMalloc((void **)&S->d_harm2, sizeof(ws60::Harm) * ws60::NH));
         CK(cudaMemcpy(S->d_harm2, hh.data(), sizeof(ws60::Harm) * ws60::NH,
@@ -976,7 +977,7 @@ static cudaError_t enqueue_search(GpuSession *S, const float2 *d_amps, double th
         w.amps = d_amps;
         w.namps = (int)S->namps;
         w.Wt = S->d_Wt;
-        w.AC = S->d_AC;
+        w.A = S->d_A;
         w.harm = S->d_harm2;
         w.chunks = S->d_chunks;
         w.tiles = S->d_tiles;

@@ -81,6 +81,10 @@ typedef struct {
     float *Wt;                 /* nrows * m */
     float *AC;                 /* nrows * 4 */
     int wt_off[CS_MAX_NH];     /* first float4 of harmonic h in Wt */
+    /* carry into the next bin as a residue threshold: for the trial residue
+     * res = (t*h*pnum) mod q the phase offset dr0 + res/q reaches 1 exactly
+     * when res >= carry_res[h] (monotone in res; src/interp.c:260-262) */
+    int carry_res[CS_MAX_NH];
 } CsTables;
 
 /* Build / free the tables.  Returns 0 or -1 with a message in err. */

@@ -25,9 +25,12 @@ constexpr int M = 16;               /* interpolation taps */
 constexpr int NTHREADS = 512;
 constexpr int KPAD = 128;
 constexpr int NPAD = 128;
-constexpr int AIMG = CS_TILE_M * KPAD * 2;   /* one fp16 A image */
 constexpr int BIMG = NPAD * KPAD * 2;        /* one fp16 B image */
-constexpr int TMEM_COLS = 256;               /* two 128-column accumulators */
+/* tensor memory (512 columns): accumulators D0, D1 at columns 0 and 128;
+ * operands A0, A1 (hi: K/2 = 64 columns, then lo: 64 columns) at 256, 384 */
+constexpr int TMEM_COLS = 512;
+constexpr int TM_D = 0, TM_A = 256;
+
 
 /* ladder widths: {1,2,3,4,6} at k = 1, {2,3,4,6} above (src/boxcar.c:100-133) */
 struct WBase {
@@ -46,13 +49,14 @@ struct Harm {
     int woff;        /* row of phase 0 in AC */
     int wt_off;      /* float4 index of (tap quad 0, phase 0) in Wt */
     uint32_t pmagic; /* floor(2^32 / P) + 1, or 0 for P == 1 */
+    int carry_res;   /* residues >= this carry into the next bin */
 };
 
 struct Args {
     const float2 *amps;
     int namps;
     const float4 *Wt;
-    const float4 *AC;
+    const float2 *A;
     const Harm *harm;
     const CsChunk *chunks;
     const int *tiles;
@@ -69,20 +73,27 @@ struct Args {
     int *err;
 };
 
-/* shared memory: B hi/lo | A0 hi/lo | A1 hi/lo | barriers | tmem slot */
+/* shared memory: B hi/lo | barriers | tmem slot | harmonic headers; the
+ * rest of the SM's 256 KB stays L1 for the weight and spectrum reads */
 constexpr int SM_B = 0;
-constexpr int SM_A = 2 * BIMG;
-constexpr int SM_BAR = SM_A + 4 * AIMG;
+constexpr int SM_BAR = 2 * BIMG;
 constexpr int SM_TM = SM_BAR + 64;
 constexpr int SM_HARM = SM_TM + 16;
 constexpr int SMEM_BYTES = SM_HARM + NH * (int)sizeof(Harm);
 
 template <class WS>
 struct Scan {
-    float hist[WS::wmax + 1];   /* hist[j] = P[i - j] */
+    float hist[WS::wmax + 2];   /* hist[j] = P[i - j] */
     float mx[WS::n];
     float P, tot;
 };
+
+static __device__ __forceinline__ float fmax3(float a, float b, float c)
+{
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
 
 template <class WS>
 static __device__ __forceinline__ void scan_init(Scan<WS> &s)
@@ -90,7 +101,7 @@ static __device__ __forceinline__ void scan_init(Scan<WS> &s)
     s.P = 0.0f;
     s.tot = 0.0f;
 #pragma unroll
-    for (int j = 0; j <= WS::wmax; j++) s.hist[j] = 0.0f;
+    for (int j = 0; j <= WS::wmax + 1; j++) s.hist[j] = 0.0f;
 #pragma unroll
     for (int a = 0; a < WS::n; a++) s.mx[a] = -INFINITY;
 }
@@ -104,7 +115,7 @@ static __device__ __forceinline__ void scan_push(Scan<WS> &s, float x, int i)
 {
     s.P = __fadd_rn(s.P, x);
 #pragma unroll
-    for (int j = WS::wmax; j > 0; j--) s.hist[j] = s.hist[j - 1];
+    for (int j = WS::wmax + 1; j > 0; j--) s.hist[j] = s.hist[j - 1];
     s.hist[0] = s.P;
     if (i == NK) s.tot = s.P;
 #pragma unroll
@@ -112,6 +123,33 @@ static __device__ __forceinline__ void scan_push(Scan<WS> &s, float x, int i)
         const int w = WS::w(a);
         const int p = i - w + 1;
         if (p >= 1 && p <= NK) s.mx[a] = fmaxf(s.mx[a], __fsub_rn(s.hist[0], s.hist[w]));
+    }
+}
+
+/* Steps i and i+1 together: both window differences of each width feed one
+ * three-input max (max is exact, so the grouping does not change results). */
+template <int NK, class WS>
+static __device__ __forceinline__ void scan_push2(Scan<WS> &s, float x0, float x1, int i)
+{
+    s.P = __fadd_rn(s.P, x0);
+    const float p1 = s.P;
+    s.P = __fadd_rn(s.P, x1);
+#pragma unroll
+    for (int j = WS::wmax + 1; j > 1; j--) s.hist[j] = s.hist[j - 2];
+    s.hist[1] = p1;
+    s.hist[0] = s.P;
+    if (i == NK) s.tot = p1;
+    if (i + 1 == NK) s.tot = s.P;
+#pragma unroll
+    for (int a = 0; a < WS::n; a++) {
+        const int w = WS::w(a);
+        const int q0 = i - w + 1, q1 = q0 + 1;      /* window starts of steps i, i+1 */
+        const bool v0 = q0 >= 1 && q0 <= NK, v1 = q1 >= 1 && q1 <= NK;
+        const float d0 = __fsub_rn(s.hist[1], s.hist[w + 1]);
+        const float d1 = __fsub_rn(s.hist[0], s.hist[w]);
+        if (v0 && v1) s.mx[a] = fmax3(s.mx[a], d0, d1);
+        else if (v0) s.mx[a] = fmaxf(s.mx[a], d0);
+        else if (v1) s.mx[a] = fmaxf(s.mx[a], d1);
     }
 }
 
@@ -140,16 +178,19 @@ static __device__ __forceinline__ float base_metric(uint32_t trow, const float *
         float v[32];
         tmem_ld32(trow + 32 * c, v);
 #pragma unroll
-        for (int u = 0; u < 32; u++) {
+        for (int u = 0; u < 32; u += 2) {
             const int i = 32 * c + u + 1;
-            if (i <= NB) {
+            if (i + 1 <= NB) {
                 if (i - 1 < WBase::wmax) first[i - 1] = v[u];
-                scan_push<NB, WBase>(s, v[u], i);
+                if (i < WBase::wmax) first[i] = v[u + 1];
+                scan_push2<NB, WBase>(s, v[u], v[u + 1], i);
             }
         }
     }
+    static_assert(NB % 2 == 0 && WBase::wmax % 2 == 0, "pairwise scan");
 #pragma unroll
-    for (int u = 0; u < WBase::wmax; u++) scan_push<NB, WBase>(s, first[u], NB + 1 + u);
+    for (int u = 0; u < WBase::wmax; u += 2)
+        scan_push2<NB, WBase>(s, first[u], first[u + 1], NB + 1 + u);
     return scan_finish<NB>(s, invsw);
 }
 
@@ -177,12 +218,12 @@ static __device__ __forceinline__ float fold_metric(uint32_t trow, const float *
     Scan<WDec> s;
     scan_init(s);
 #pragma unroll
-    for (int j = 0; j < NK; j++) {
-        r[j] = __fmul_rn(r[j], invk);
-        scan_push<NK, WDec>(s, r[j], j + 1);
-    }
+    for (int j = 0; j < NK; j++) r[j] = __fmul_rn(r[j], invk);
+    static_assert(NK % 2 == 0 && WDec::wmax % 2 == 0, "pairwise scan");
 #pragma unroll
-    for (int u = 0; u < WDec::wmax; u++) scan_push<NK, WDec>(s, r[u], NK + 1 + u);
+    for (int j = 0; j < NK; j += 2) scan_push2<NK, WDec>(s, r[j], r[j + 1], j + 1);
+#pragma unroll
+    for (int u = 0; u < WDec::wmax; u += 2) scan_push2<NK, WDec>(s, r[u], r[u + 1], NK + 1 + u);
     return scan_finish<NK>(s, invsw);
 }
 
@@ -205,6 +246,26 @@ static __device__ __forceinline__ void emit(const Args &a, bool hit, int ci, int
             a.recs[pos] = rec;
         }
     }
+}
+
+/* 4 consecutive 32-bit tensor-memory columns of this warp's 32 lanes */
+static __device__ __forceinline__ void tmem_st4(uint32_t taddr, uint32_t a, uint32_t b,
+                                                uint32_t c, uint32_t d)
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};"
+                 :: "r"(taddr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
+}
+
+/* D[tmem] (+)= A[tmem] * B[smem]^T, 128 x N x 16, fp16 in, fp32 accumulate */
+static __device__ __forceinline__ void mma_f16_ts(uint32_t d_tmem, uint32_t a_tmem,
+                                                  uint64_t bdesc, uint32_t idesc,
+                                                  uint32_t accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}"
+                 :: "r"(d_tmem), "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate)
+                 : "memory");
 }
 
 static __device__ __forceinline__ void mbar_arrive(uint32_t bar)
@@ -256,13 +317,6 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const Args a)
     {
         uint4 *dst = reinterpret_cast<uint4 *>(smem + SM_B);
         for (int i = tid; i < (2 * BIMG) / 16; i += NTHREADS) dst[i] = a.bimg[i];
-        /* the K padding block (k = 120..127) of both A buffers stays zero */
-        for (int i = tid; i < 4 * CS_TILE_M; i += NTHREADS) {
-            const int img = i / CS_TILE_M, r = i % CS_TILE_M;
-            const uint32_t off = (uint32_t)img * AIMG + 15u * (CS_TILE_M * 16) +
-                                 (uint32_t)(r >> 3) * 128 + (uint32_t)(r & 7) * 16;
-            *reinterpret_cast<uint4 *>(smem + SM_A + off) = make_uint4(0, 0, 0, 0);
-        }
     }
     fence_proxy_async();
     tc_fence_before();
@@ -271,18 +325,34 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const Args a)
     const uint32_t tmem = *tm_slot;
     const float scale = operand_scale(a.amax, a.gbound);
     const float inv_scale = 1.0f / scale;
+    /* each CTA owns a contiguous run of tiles: neighbouring tiles read the
+     * same spectral windows and weight rows, which then stay in L1 */
+    const int per_cta = (a.ntiles + gridDim.x - 1) / gridDim.x;
+    const int tile_begin = min(a.ntiles, (int)blockIdx.x * per_cta);
+    const int tile_end = min(a.ntiles, tile_begin + per_cta);
 
     if (warp < 8) {
         /* ------------------------- interpolation ------------------------- */
         const int r = tid & (CS_TILE_M - 1);
         const int par = tid >> 7;
+        const uint32_t tlane = (uint32_t)((warp & 3) * 32) << 16;
+        if (par == 1) {
+            /* the K padding block (k = 120..127) of both A buffers stays zero */
+#pragma unroll
+            for (int b = 0; b < 2; b++) {
+                const uint32_t ab = tmem + tlane + (uint32_t)(TM_A + 128 * b);
+                tmem_st4(ab + 60, 0, 0, 0, 0);
+                tmem_st4(ab + 64 + 60, 0, 0, 0, 0);
+            }
+        }
         int it = 0;
-        for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, it++) {
+        for (int tile = tile_begin; tile < tile_end; tile++, it++) {
             const int s = it & 1;
             if (it >= 2 && !mbar_wait(bar_aempty + 8 * s, ((it - 2) >> 1) & 1)) {
                 if (lane == 0) atomicExch(a.err, 1);
                 break;
             }
+            tc_fence_after();
             const int ci = a.tiles[3 * tile], j0 = a.tiles[3 * tile + 1];
             const int cnt = a.tiles[3 * tile + 2];
             const CsChunk &ch = a.chunks[ci];
@@ -297,19 +367,65 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const Args a)
                 Q = (uint32_t)(tp / (unsigned)a.q);
                 R = (uint32_t)(tp - (unsigned long long)Q * (unsigned)a.q);
             }
-            /* residue/quotient of t*h*pnum for h = 4*par+1, and the steps +1, +5 */
-            uint32_t res, qint, q5, r5;
+            /* residue/quotient of t*h*pnum for h = 4*par+1, and the steps +1, +4 */
+            uint32_t res, qint, q4, r4;
             {
                 const uint32_t h0 = 4u * par + 1u;
                 uint32_t qd;
                 divmod_q(h0 * R, (uint32_t)a.q, a.qmagic, qd, res);
                 qint = h0 * Q + qd;
-                divmod_q(5u * R, (uint32_t)a.q, a.qmagic, qd, r5);
-                q5 = 5u * Q + qd;
+                divmod_q(4u * R, (uint32_t)a.q, a.qmagic, qd, r4);
+                q4 = 4u * Q + qd;
             }
-            unsigned char *abuf = smem + SM_A + s * 2 * AIMG;
+            const uint32_t abuf = tmem + tlane + (uint32_t)(TM_A + 128 * s);
             for (int hb = par; hb < NH / 4; hb += 2) {
                 uint32_t hw[4], lw[4];
+                const bool full = valid && (((filled >> (4 * hb)) & 0xFULL) == 0xFULL);
+                if (full) {
+                    /* every harmonic of the block is active: no branches, so the
+                     * loads of all four harmonics can be in flight together */
+                    float xr4[4], xi4[4];
+                    uint32_t rr = res, qq = qint;
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const Harm hm = hs[4 * hb + u];
+                        const uint32_t ph = mod_magic(t, (uint32_t)hm.P, hm.pmagic);
+                        const int b0 = hm.rfloor0 + (int)qq + ((int)rr >= hm.carry_res ? 1 : 0) +
+                                       1 - M / 2;
+                        /* in range by construction for active harmonics; clamp for safety */
+                        const int bs = min(max(b0, 0), a.namps - M);
+                        const float2 *ap = a.amps + bs;
+                        const float4 *wq = a.Wt + hm.wt_off + ph;
+                        float ar = 0.0f, ai = 0.0f;
+#pragma unroll
+                        for (int i4 = 0; i4 < M / 4; i4++) {
+                            const float4 w = __ldg(wq + i4 * hm.P);
+                            const float2 v0 = __ldg(ap + 4 * i4), v1 = __ldg(ap + 4 * i4 + 1);
+                            const float2 v2 = __ldg(ap + 4 * i4 + 2), v3 = __ldg(ap + 4 * i4 + 3);
+                            ar = __fmaf_rn(w.x, v0.x, ar); ai = __fmaf_rn(w.x, v0.y, ai);
+                            ar = __fmaf_rn(w.y, v1.x, ar); ai = __fmaf_rn(w.y, v1.y, ai);
+                            ar = __fmaf_rn(w.z, v2.x, ar); ai = __fmaf_rn(w.z, v2.y, ai);
+                            ar = __fmaf_rn(w.w, v3.x, ar); ai = __fmaf_rn(w.w, v3.y, ai);
+                        }
+                        const float2 g = __ldg(a.A + hm.woff + ph);
+                        const bool inb = (b0 == bs);
+                        xr4[u] = inb ? __fsub_rn(__fmul_rn(g.x, ar), __fmul_rn(g.y, ai)) : 0.0f;
+                        xi4[u] = inb ? __fadd_rn(__fmul_rn(g.x, ai), __fmul_rn(g.y, ar)) : 0.0f;
+                        rr += R; qq += Q;
+                        if (rr >= (uint32_t)a.q) { rr -= (uint32_t)a.q; qq += 1; }
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const float2 sc = make_float2(xr4[u] * scale, xi4[u] * scale);
+                        const __half2 hi = __float22half2_rn(sc);
+                        const float2 back = __half22float2(hi);
+                        const __half2 lo = __float22half2_rn(
+                            make_float2(__fsub_rn(sc.x, back.x), __fsub_rn(sc.y, back.y)));
+                        hw[u] = *reinterpret_cast<const uint32_t *>(&hi);
+                        lw[u] = *reinterpret_cast<const uint32_t *>(&lo);
+                    }
+                    res = rr; qint = qq;
+                } else
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
                     const int h = 4 * hb + u + 1;
@@ -317,8 +433,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const Args a)
                     if (valid && ((filled >> (h - 1)) & 1ULL)) {
                         const Harm hm = hs[h - 1];
                         const uint32_t ph = mod_magic(t, (uint32_t)hm.P, hm.pmagic);
-                        const float4 ac = __ldg(a.AC + hm.woff + ph);
-                        const int base = hm.rfloor0 + (int)qint + __float_as_int(ac.z);
+                        const int base = hm.rfloor0 + (int)qint + ((int)res >= hm.carry_res ? 1 : 0);
                         const int b0 = base + 1 - M / 2;
                         float ar = 0.0f, ai = 0.0f;
                         if ((unsigned)b0 <= (unsigned)(a.namps - M)) {
@@ -335,8 +450,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const Args a)
                                 ar = __fmaf_rn(w.w, v3.x, ar); ai = __fmaf_rn(w.w, v3.y, ai);
                             }
                         }
-                        xr = __fsub_rn(__fmul_rn(ac.x, ar), __fmul_rn(ac.y, ai));
-                        xi = __fadd_rn(__fmul_rn(ac.x, ai), __fmul_rn(ac.y, ar));
+                        const float2 g = __ldg(a.A + hm.woff + ph);
+                        xr = __fsub_rn(__fmul_rn(g.x, ar), __fmul_rn(g.y, ai));
+                        xi = __fadd_rn(__fmul_rn(g.x, ai), __fmul_rn(g.y, ar));
                     }
                     const float2 sc = make_float2(xr * scale, xi * scale);
                     const __half2 hi = __float22half2_rn(sc);
@@ -345,20 +461,18 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const Args a)
                         make_float2(__fsub_rn(sc.x, back.x), __fsub_rn(sc.y, back.y)));
                     hw[u] = *reinterpret_cast<const uint32_t *>(&hi);
                     lw[u] = *reinterpret_cast<const uint32_t *>(&lo);
-                    if (u < 3) {           /* advance h -> h+1 */
-                        res += R; qint += Q;
-                        if (res >= (uint32_t)a.q) { res -= (uint32_t)a.q; qint += 1; }
-                    }
+                    res += R; qint += Q;   /* h -> h+1 */
+                    if (res >= (uint32_t)a.q) { res -= (uint32_t)a.q; qint += 1; }
                 }
-                /* h -> h+5: from 4hb+4 to the first harmonic of block hb+2 */
-                res += r5; qint += q5;
+                /* both paths leave the state at 4hb+5; +4 more reaches block hb+2 */
+                res += r4; qint += q4;
                 if (res >= (uint32_t)a.q) { res -= (uint32_t)a.q; qint += 1; }
-                const uint32_t off = (uint32_t)hb * (CS_TILE_M * 16) + (uint32_t)(r >> 3) * 128 +
-                                     (uint32_t)(r & 7) * 16;
-                *reinterpret_cast<uint4 *>(abuf + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-                *reinterpret_cast<uint4 *>(abuf + AIMG + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                /* K block hb = columns 4hb..4hb+3 (two halves per column) */
+                tmem_st4(abuf + 4 * hb, hw[0], hw[1], hw[2], hw[3]);
+                tmem_st4(abuf + 64 + 4 * hb, lw[0], lw[1], lw[2], lw[3]);
             }
-            fence_proxy_async();
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(bar_afull + 8 * s);
         }
@@ -370,7 +484,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const Args a)
         const bool leader = (warp == 8 && lane == 0);
         const uint32_t idesc = (1u << 4) | ((uint32_t)(NPAD >> 3) << 17) |
                                ((uint32_t)(CS_TILE_M >> 4) << 24);
-        const uint32_t lbo_a = CS_TILE_M * 16, lbo_b = NPAD * 16;
+        const uint32_t lbo_b = NPAD * 16;
         const uint32_t b_hi = smem_u32(smem + SM_B), b_lo = b_hi + BIMG;
         int issued = 0, consumed = 0;
         bool ok = true;
@@ -379,8 +493,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const Args a)
             const int s = it & 1;
             if (!mbar_wait(bar_afull + 8 * s, (it >> 1) & 1)) return false;
             tc_fence_after();
-            const uint32_t a_hi = smem_u32(smem + SM_A + s * 2 * AIMG), a_lo = a_hi + AIMG;
-            const uint32_t d = tmem + (uint32_t)(s * 128);
+            const uint32_t a_hi = tmem + (uint32_t)(TM_A + 128 * s), a_lo = a_hi + 64;
+            const uint32_t d = tmem + (uint32_t)(TM_D + 128 * s);
             uint32_t acc = 0;
 #pragma unroll
             for (int pass = 0; pass < 3; pass++) {
@@ -388,8 +502,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const Args a)
                 const uint32_t bbase = (pass == 2) ? b_lo : b_hi;
 #pragma unroll
                 for (int k = 0; k < KPAD / 16; k++) {
-                    mma_f16(d, umma_desc(abase + (uint32_t)k * 2 * lbo_a, lbo_a, 128),
-                            umma_desc(bbase + (uint32_t)k * 2 * lbo_b, lbo_b, 128), idesc, acc);
+                    mma_f16_ts(d, abase + (uint32_t)(8 * k),
+                               umma_desc(bbase + (uint32_t)k * 2 * lbo_b, lbo_b, 128), idesc, acc);
                     acc = 1;
                 }
             }
@@ -398,15 +512,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const Args a)
             return true;
         };
 
-        if (leader && (int)blockIdx.x < a.ntiles) {
+        if (leader && tile_begin < tile_end) {
             ok = issue(0);
             if (ok) issued = 1;
             else atomicExch(a.err, 1);
         }
         int it = 0;
-        for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, it++) {
+        for (int tile = tile_begin; tile < tile_end; tile++, it++) {
             const int s = it & 1;
-            if (leader && ok && tile + (int)gridDim.x < a.ntiles) {
+            if (leader && ok && tile + 1 < tile_end) {
                 ok = issue(it + 1);
                 if (ok) issued++;
                 else atomicExch(a.err, 1);
@@ -424,7 +538,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const Args a)
             const CsChunk &ch = a.chunks[ci];
             const bool valid = r < cnt;
             const int j = j0 + r;
-            const uint32_t trow = tmem + (uint32_t)(s * 128) + ((uint32_t)(quarter * 32) << 16);
+            const uint32_t trow = tmem + (uint32_t)(TM_D + s * 128) + ((uint32_t)(quarter * 32) << 16);
             if (grp == 0) {
                 float iv[5], iw[4];
 #pragma unroll

@@ -268,6 +268,23 @@ CS_HIDDEN_API int cs_tables_build(CsTables *t, const FFTFile *ft, const SearchPa
     /* pad the bound by 1% for the FP32 rounding of the accumulation */
     t->gbound = (float)(gmax * 1.01 + 1e-30);
 
+    /* carry thresholds, with the reference's expression for the offset */
+    for (h = 1; h <= nh; h++) {
+        const DirectPlan *dp = &dplans->plans[h - 1];
+        int res = 0;
+        while (res < t->q && !(dp->dr0 + (double)res / (double)t->q >= 1.0)) res++;
+        t->carry_res[h - 1] = res;
+        /* cross-check against the tabulated carries */
+        int rr;
+        for (rr = 0; rr < t->q; rr++) {
+            const int row = dp->row[rr];
+            if (row > 0 && (int)dp->carry[row - 1] != (rr >= res)) {
+                snprintf(err, errlen, "carry of harmonic %d is not monotone in the residue", h);
+                return -1;
+            }
+        }
+    }
+
     /* transposed weights and packed phase factor + carry */
     t->Wt = (float *)malloc((size_t)nrows * t->m * sizeof(float));
     t->AC = (float *)malloc((size_t)nrows * 4 * sizeof(float));
