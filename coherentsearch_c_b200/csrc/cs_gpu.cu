@@ -117,6 +117,7 @@ static __device__ bool mbar_wait(uint32_t bar, uint32_t parity)
     const unsigned long long t0 = global_ns();
     while (!mbar_try(bar, parity)) {
         if (global_ns() - t0 > CS_WAIT_NS) return false;
+        __nanosleep(64);     /* leave the issue slots to the working warps */
     }
     return true;
 }
@@ -648,6 +649,7 @@ struct GpuSession {
     float4 *d_Wt;
     float4 *d_AC;
     ws60::Harm *d_harm2;
+    ws60::Harm hh[ws60::NH];
 };
 
 static cudaError_t select_device(int device)
@@ -786,6 +788,7 @@ static int ws60_applies(const CsTables &t, long long total)
     for (int h = 0; h < t.nh; h++) rmax = std::max(rmax, (double)t.harm[h].rfloor0);
     if (rmax + tmax * t.nh * (double)t.pnum / (double)t.q + 64 >= 2147483647.0) return 0;
     if ((double)t.q * 5.0 * t.q >= 4294967295.0) return 0;
+    for (int h = 0; h < t.nh; h++) if (t.harm[h].P > ws60::WT_STRIDE) return 0;
     return 1;
 }
 
@@ -876,24 +879,27 @@ CS_EXPORT GpuSession *cs_gpu_session_create(const FFTFile *ft, const SearchParam
     S->use_ws = ws60_applies(S->tab, total) && S->namps < 2147483000LL &&
                 ws60::SMEM_BYTES <= S->max_smem;
     if (S->use_ws) {
-        std::vector<ws60::Harm> hh(ws60::NH);
+        /* weights: harmonic h, tap quad i4, phase p at float4
+         * h*4*WT_STRIDE + i4*WT_STRIDE + p */
+        const size_t nq = (size_t)ws60::NH * 4 * ws60::WT_STRIDE;
+        std::vector<float> wfix(nq * 4, 0.0f);
         for (int h = 0; h < ws60::NH; h++) {
-            hh[h].rfloor0 = (int)S->tab.harm[h].rfloor0;
-            hh[h].P = S->tab.harm[h].P;
-            hh[h].woff = S->tab.harm[h].woff;
-            hh[h].wt_off = S->tab.wt_off[h];
-            hh[h].pmagic = magic_for(S->tab.harm[h].P);
-            hh[h].carry_res = S->tab.carry_res[h];
+            S->hh[h].rfloor0 = (int)S->tab.harm[h].rfloor0;
+            S->hh[h].P = S->tab.harm[h].P;
+            S->hh[h].woff = S->tab.harm[h].woff;
+            S->hh[h].wt_off = h * 4 * ws60::WT_STRIDE;
+            S->hh[h].pmagic = magic_for(S->tab.harm[h].P);
+            S->hh[h].carry_res = S->tab.carry_res[h];
+            const int P = S->tab.harm[h].P, off = S->tab.harm[h].woff;
+            for (int ph = 0; ph < P; ph++)
+                for (int i = 0; i < ws60::M; i++)
+                    wfix[4 * ((size_t)h * 4 * ws60::WT_STRIDE + (i / 4) * ws60::WT_STRIDE + ph) + (i & 3)] =
+                        S->tab.W[(size_t)(off + ph) * S->tab.m + i];
         }
         CK(cudaMalloc((void **)&S->d_harm2, sizeof(ws60::Harm) * ws60::NH));
-        CK(cudaMemcpy(S->d_harm2, hh.data(), sizeof(ws60::Harm) * ws60::NH,
-                      cudaMemcpyHostToDevice));
-        CK(cudaMalloc((void **)&S->d_Wt, (size_t)S->tab.nrows * S->tab.m * sizeof(float)));
-        CK(cudaMemcpy(S->d_Wt, S->tab.Wt, (size_t)S->tab.nrows * S->tab.m * sizeof(float),
-                      cudaMemcpyHostToDevice));
-        CK(cudaMalloc((void **)&S->d_AC, (size_t)S->tab.nrows * 4 * sizeof(float)));
-        CK(cudaMemcpy(S->d_AC, S->tab.AC, (size_t)S->tab.nrows * 4 * sizeof(float),
-                      cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(S->d_harm2, S->hh, sizeof(ws60::Harm) * ws60::NH, cudaMemcpyHostToDevice));
+        CK(cudaMalloc((void **)&S->d_Wt, nq * sizeof(float4)));
+        CK(cudaMemcpy(S->d_Wt, wfix.data(), nq * sizeof(float4), cudaMemcpyHostToDevice));
         CK(cudaFuncSetAttribute(ws60::search_ws60, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 ws60::SMEM_BYTES));
     }

@@ -30,6 +30,10 @@ constexpr int BIMG = NPAD * KPAD * 2;        /* one fp16 B image */
  * operands A0, A1 (hi: K/2 = 64 columns, then lo: 64 columns) at 256, 384 */
 constexpr int TMEM_COLS = 512;
 constexpr int TM_D = 0, TM_A = 256;
+/* float4 stride between the tap quads of one harmonic in the weight table
+ * (the largest phase-cycle length the kernel accepts, so the four loads of
+ * a row use immediate offsets) */
+constexpr int WT_STRIDE = 128;
 
 
 /* ladder widths: {1,2,3,4,6} at k = 1, {2,3,4,6} above (src/boxcar.c:100-133) */
@@ -294,7 +298,7 @@ static __device__ __forceinline__ uint32_t mod_magic(uint32_t t, uint32_t P, uin
     return t - pr;
 }
 
-__global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const Args a)
+__global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const __grid_constant__ Args a)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -305,6 +309,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const Args a)
     Harm *hs = reinterpret_cast<Harm *>(smem + SM_HARM);
 
     if (warp == 0) tmem_alloc(smem_u32(tm_slot), TMEM_COLS);
+    for (int h = tid; h < NH; h += NTHREADS) hs[h] = a.harm[h];
     if (tid == 0) {
         mbar_init(bar_afull, 8);
         mbar_init(bar_afull + 8, 8);
@@ -313,7 +318,6 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const Args a)
         mbar_init(bar_dfull, 1);
         mbar_init(bar_dfull + 8, 1);
     }
-    for (int h = tid; h < NH; h += NTHREADS) hs[h] = a.harm[h];
     {
         uint4 *dst = reinterpret_cast<uint4 *>(smem + SM_B);
         for (int i = tid; i < (2 * BIMG) / 16; i += NTHREADS) dst[i] = a.bimg[i];
@@ -396,17 +400,20 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const Args a)
                         const int bs = min(max(b0, 0), a.namps - M);
                         const float2 *ap = a.amps + bs;
                         const float4 *wq = a.Wt + hm.wt_off + ph;
-                        float ar = 0.0f, ai = 0.0f;
+                        /* packed FP32: each lane of __ffma2_rn is a correctly rounded
+                         * fma, so (Re, Im) advance exactly as two scalar chains */
+                        float2 acc = make_float2(0.0f, 0.0f);
 #pragma unroll
                         for (int i4 = 0; i4 < M / 4; i4++) {
-                            const float4 w = __ldg(wq + i4 * hm.P);
+                            const float4 w = __ldg(wq + i4 * WT_STRIDE);
                             const float2 v0 = __ldg(ap + 4 * i4), v1 = __ldg(ap + 4 * i4 + 1);
                             const float2 v2 = __ldg(ap + 4 * i4 + 2), v3 = __ldg(ap + 4 * i4 + 3);
-                            ar = __fmaf_rn(w.x, v0.x, ar); ai = __fmaf_rn(w.x, v0.y, ai);
-                            ar = __fmaf_rn(w.y, v1.x, ar); ai = __fmaf_rn(w.y, v1.y, ai);
-                            ar = __fmaf_rn(w.z, v2.x, ar); ai = __fmaf_rn(w.z, v2.y, ai);
-                            ar = __fmaf_rn(w.w, v3.x, ar); ai = __fmaf_rn(w.w, v3.y, ai);
+                            acc = __ffma2_rn(make_float2(w.x, w.x), v0, acc);
+                            acc = __ffma2_rn(make_float2(w.y, w.y), v1, acc);
+                            acc = __ffma2_rn(make_float2(w.z, w.z), v2, acc);
+                            acc = __ffma2_rn(make_float2(w.w, w.w), v3, acc);
                         }
+                        const float ar = acc.x, ai = acc.y;
                         const float2 g = __ldg(a.A + hm.woff + ph);
                         const bool inb = (b0 == bs);
                         xr4[u] = inb ? __fsub_rn(__fmul_rn(g.x, ar), __fmul_rn(g.y, ai)) : 0.0f;
@@ -441,7 +448,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const Args a)
                             const float4 *wq = a.Wt + hm.wt_off + ph;
 #pragma unroll
                             for (int i4 = 0; i4 < M / 4; i4++) {
-                                const float4 w = __ldg(wq + i4 * hm.P);
+                                const float4 w = __ldg(wq + i4 * WT_STRIDE);
                                 const float2 v0 = __ldg(ap + 4 * i4), v1 = __ldg(ap + 4 * i4 + 1);
                                 const float2 v2 = __ldg(ap + 4 * i4 + 2), v3 = __ldg(ap + 4 * i4 + 3);
                                 ar = __fmaf_rn(w.x, v0.x, ar); ai = __fmaf_rn(w.x, v0.y, ai);
