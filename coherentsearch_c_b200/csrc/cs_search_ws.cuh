@@ -3,13 +3,15 @@
  * (nharms = 60, m = 16, k = 1..6, ladder widths {1,2,3,4,6} / {2,3,4,6}).
  *
  * One persistent CTA per SM, 16 warps:
- *   warps 0-7   interpolation: tile i -> fp16 hi/lo A operand in shared
- *               memory buffer i%2 (same FP32 arithmetic as the generic
- *               kernel, bit-identical harmonic amplitudes);
- *   warps 8-15  tensor-core issue (one elected thread) and the boxcar
- *               epilogue of tile i from tensor-memory accumulator i%2 while
- *               the interpolation warps fill the other A buffer.
- * Hand-off through mbarriers: a_full (8 warp arrivals), a_empty and d_full
+ *   warps 0-7   interpolation of harmonic blocks 0..HEAD-1 of tile i into
+ *               the fp16 hi/lo A operand in tensor-memory buffer i%2 (same
+ *               FP32 arithmetic as the generic kernel, bit-identical
+ *               harmonic amplitudes);
+ *   warps 8-15  the remaining harmonic blocks of tile i+1, tensor-core issue
+ *               (one elected thread), then the boxcar epilogue of tile i from
+ *               tensor-memory accumulator i%2.  The split evens out the two
+ *               roles' instruction counts per tile.
+ * Hand-off through mbarriers: a_full (16 warp arrivals), a_empty and d_full
  * (tcgen05.commit).  The epilogue keeps every prefix sum in registers: with
  * the bin count and widths known at compile time, the cyclic prefix, the
  * sliding window differences P[i] - P[i-w] and the k-fold sums all unroll
@@ -298,6 +300,138 @@ static __device__ __forceinline__ uint32_t mod_magic(uint32_t t, uint32_t P, uin
     return t - pr;
 }
 
+
+constexpr int HEAD = 12;            /* blocks 0..HEAD-1: interpolation warps */
+constexpr int G0 = 2;               /* blocks HEAD..HEAD+G0-1: epilogue group 0; rest group 1 */
+
+struct TrialState {
+    uint32_t t, Q, R;               /* trial index, t*pnum = Q*q + R */
+    bool valid;
+    unsigned long long filled;
+};
+
+static __device__ __forceinline__ TrialState trial_state(const Args &a, int tile, int r)
+{
+    TrialState ts;
+    const int ci = a.tiles[3 * tile], j0 = a.tiles[3 * tile + 1];
+    const int cnt = a.tiles[3 * tile + 2];
+    const CsChunk &ch = a.chunks[ci];
+    ts.filled = ch.filled;
+    ts.valid = r < cnt;
+    ts.t = (uint32_t)(ch.i0 + j0 + r);
+    if (a.pnum == 1) {
+        divmod_q(ts.t, (uint32_t)a.q, a.qmagic, ts.Q, ts.R);
+    } else {
+        const unsigned long long tp = (unsigned long long)ts.t * (unsigned)a.pnum;
+        ts.Q = (uint32_t)(tp / (unsigned)a.q);
+        ts.R = (uint32_t)(tp - (unsigned long long)ts.Q * (unsigned)a.q);
+    }
+    return ts;
+}
+
+/* residue and quotient of t*h*pnum over q (h <= 60, so h*R < 2^32) */
+static __device__ __forceinline__ void state_at(const Args &a, const TrialState &ts, uint32_t h,
+                                                uint32_t &res, uint32_t &qint)
+{
+    uint32_t qd;
+    divmod_q(h * ts.R, (uint32_t)a.q, a.qmagic, qd, res);
+    qint = h * ts.Q + qd;
+}
+
+/* Interpolate harmonics 4hb+1..4hb+4 of one trial (src/cuda.cu:120-135
+ * arithmetic) and store them, split into fp16 hi/lo, as K block hb of the
+ * A operand in tensor memory.  (res, qint) enter at h = 4hb+1 and leave at
+ * h = 4hb+5. */
+static __device__ __forceinline__ void interp_block(const Args &a, const Harm *hs,
+                                                    const TrialState &ts, int hb,
+                                                    uint32_t &res, uint32_t &qint,
+                                                    float scale, uint32_t abuf)
+{
+    const uint32_t t = ts.t, R = ts.R, Q = ts.Q;
+    uint32_t hw[4], lw[4];
+    const bool full = ts.valid && (((ts.filled >> (4 * hb)) & 0xFULL) == 0xFULL);
+    float xr4[4], xi4[4];
+    if (full) {
+        /* every harmonic of the block is active: no branches, so the loads of
+         * all four harmonics can be in flight together */
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const Harm hm = hs[4 * hb + u];
+            const uint32_t ph = mod_magic(t, (uint32_t)hm.P, hm.pmagic);
+            const int b0 = hm.rfloor0 + (int)qint + ((int)res >= hm.carry_res ? 1 : 0) + 1 - M / 2;
+            /* in range by construction for active harmonics; clamp for safety */
+            const int bs = min(max(b0, 0), a.namps - M);
+            const float2 *ap = a.amps + bs;
+            const float4 *wq = a.Wt + hm.wt_off + ph;
+            /* packed FP32: each lane of __ffma2_rn is a correctly rounded fma,
+             * so (Re, Im) advance exactly as two scalar chains */
+            float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll
+            for (int i4 = 0; i4 < M / 4; i4++) {
+                const float4 w = __ldg(wq + i4 * WT_STRIDE);
+                const float2 v0 = __ldg(ap + 4 * i4), v1 = __ldg(ap + 4 * i4 + 1);
+                const float2 v2 = __ldg(ap + 4 * i4 + 2), v3 = __ldg(ap + 4 * i4 + 3);
+                acc = __ffma2_rn(make_float2(w.x, w.x), v0, acc);
+                acc = __ffma2_rn(make_float2(w.y, w.y), v1, acc);
+                acc = __ffma2_rn(make_float2(w.z, w.z), v2, acc);
+                acc = __ffma2_rn(make_float2(w.w, w.w), v3, acc);
+            }
+            const float2 g = __ldg(a.A + hm.woff + ph);
+            const bool inb = (b0 == bs);
+            xr4[u] = inb ? __fsub_rn(__fmul_rn(g.x, acc.x), __fmul_rn(g.y, acc.y)) : 0.0f;
+            xi4[u] = inb ? __fadd_rn(__fmul_rn(g.x, acc.y), __fmul_rn(g.y, acc.x)) : 0.0f;
+            res += R; qint += Q;
+            if (res >= (uint32_t)a.q) { res -= (uint32_t)a.q; qint += 1; }
+        }
+    } else {
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int h = 4 * hb + u + 1;
+            float xr = 0.0f, xi = 0.0f;
+            if (ts.valid && ((ts.filled >> (h - 1)) & 1ULL)) {
+                const Harm hm = hs[h - 1];
+                const uint32_t ph = mod_magic(t, (uint32_t)hm.P, hm.pmagic);
+                const int b0 = hm.rfloor0 + (int)qint + ((int)res >= hm.carry_res ? 1 : 0) + 1 - M / 2;
+                float ar = 0.0f, ai = 0.0f;
+                if ((unsigned)b0 <= (unsigned)(a.namps - M)) {
+                    const float2 *ap = a.amps + b0;
+                    const float4 *wq = a.Wt + hm.wt_off + ph;
+#pragma unroll
+                    for (int i4 = 0; i4 < M / 4; i4++) {
+                        const float4 w = __ldg(wq + i4 * WT_STRIDE);
+                        const float2 v0 = __ldg(ap + 4 * i4), v1 = __ldg(ap + 4 * i4 + 1);
+                        const float2 v2 = __ldg(ap + 4 * i4 + 2), v3 = __ldg(ap + 4 * i4 + 3);
+                        ar = __fmaf_rn(w.x, v0.x, ar); ai = __fmaf_rn(w.x, v0.y, ai);
+                        ar = __fmaf_rn(w.y, v1.x, ar); ai = __fmaf_rn(w.y, v1.y, ai);
+                        ar = __fmaf_rn(w.z, v2.x, ar); ai = __fmaf_rn(w.z, v2.y, ai);
+                        ar = __fmaf_rn(w.w, v3.x, ar); ai = __fmaf_rn(w.w, v3.y, ai);
+                    }
+                }
+                const float2 g = __ldg(a.A + hm.woff + ph);
+                xr = __fsub_rn(__fmul_rn(g.x, ar), __fmul_rn(g.y, ai));
+                xi = __fadd_rn(__fmul_rn(g.x, ai), __fmul_rn(g.y, ar));
+            }
+            xr4[u] = xr;
+            xi4[u] = xi;
+            res += R; qint += Q;
+            if (res >= (uint32_t)a.q) { res -= (uint32_t)a.q; qint += 1; }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        const float2 sc = make_float2(xr4[u] * scale, xi4[u] * scale);
+        const __half2 hi = __float22half2_rn(sc);
+        const float2 back = __half22float2(hi);
+        const __half2 lo = __float22half2_rn(
+            make_float2(__fsub_rn(sc.x, back.x), __fsub_rn(sc.y, back.y)));
+        hw[u] = *reinterpret_cast<const uint32_t *>(&hi);
+        lw[u] = *reinterpret_cast<const uint32_t *>(&lo);
+    }
+    /* K block hb = columns 4hb..4hb+3 (two halves per column) */
+    tmem_st4(abuf + 4 * hb, hw[0], hw[1], hw[2], hw[3]);
+    tmem_st4(abuf + 64 + 4 * hb, lw[0], lw[1], lw[2], lw[3]);
+}
+
 __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const __grid_constant__ Args a)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -311,8 +445,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const __grid_constant
     if (warp == 0) tmem_alloc(smem_u32(tm_slot), TMEM_COLS);
     for (int h = tid; h < NH; h += NTHREADS) hs[h] = a.harm[h];
     if (tid == 0) {
-        mbar_init(bar_afull, 8);
-        mbar_init(bar_afull + 8, 8);
+        mbar_init(bar_afull, 16);      /* 8 interpolation + 8 epilogue warps */
+        mbar_init(bar_afull + 8, 16);
         mbar_init(bar_aempty, 1);
         mbar_init(bar_aempty + 8, 1);
         mbar_init(bar_dfull, 1);
@@ -336,7 +470,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const __grid_constant
     const int tile_end = min(a.ntiles, tile_begin + per_cta);
 
     if (warp < 8) {
-        /* ------------------------- interpolation ------------------------- */
+        /* --------------- interpolation of blocks 0..HEAD-1 --------------- */
         const int r = tid & (CS_TILE_M - 1);
         const int par = tid >> 7;
         const uint32_t tlane = (uint32_t)((warp & 3) * 32) << 16;
@@ -357,126 +491,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const __grid_constant
                 break;
             }
             tc_fence_after();
-            const int ci = a.tiles[3 * tile], j0 = a.tiles[3 * tile + 1];
-            const int cnt = a.tiles[3 * tile + 2];
-            const CsChunk &ch = a.chunks[ci];
-            const unsigned long long filled = ch.filled;
-            const bool valid = r < cnt;
-            const uint32_t t = (uint32_t)(ch.i0 + j0 + r);
-            uint32_t Q, R;
-            if (a.pnum == 1) {
-                divmod_q(t, (uint32_t)a.q, a.qmagic, Q, R);
-            } else {
-                const unsigned long long tp = (unsigned long long)t * (unsigned)a.pnum;
-                Q = (uint32_t)(tp / (unsigned)a.q);
-                R = (uint32_t)(tp - (unsigned long long)Q * (unsigned)a.q);
-            }
-            /* residue/quotient of t*h*pnum for h = 4*par+1, and the steps +1, +4 */
-            uint32_t res, qint, q4, r4;
-            {
-                const uint32_t h0 = 4u * par + 1u;
-                uint32_t qd;
-                divmod_q(h0 * R, (uint32_t)a.q, a.qmagic, qd, res);
-                qint = h0 * Q + qd;
-                divmod_q(4u * R, (uint32_t)a.q, a.qmagic, qd, r4);
-                q4 = 4u * Q + qd;
-            }
+            const TrialState ts = trial_state(a, tile, r);
             const uint32_t abuf = tmem + tlane + (uint32_t)(TM_A + 128 * s);
-            for (int hb = par; hb < NH / 4; hb += 2) {
-                uint32_t hw[4], lw[4];
-                const bool full = valid && (((filled >> (4 * hb)) & 0xFULL) == 0xFULL);
-                if (full) {
-                    /* every harmonic of the block is active: no branches, so the
-                     * loads of all four harmonics can be in flight together */
-                    float xr4[4], xi4[4];
-                    uint32_t rr = res, qq = qint;
-#pragma unroll
-                    for (int u = 0; u < 4; u++) {
-                        const Harm hm = hs[4 * hb + u];
-                        const uint32_t ph = mod_magic(t, (uint32_t)hm.P, hm.pmagic);
-                        const int b0 = hm.rfloor0 + (int)qq + ((int)rr >= hm.carry_res ? 1 : 0) +
-                                       1 - M / 2;
-                        /* in range by construction for active harmonics; clamp for safety */
-                        const int bs = min(max(b0, 0), a.namps - M);
-                        const float2 *ap = a.amps + bs;
-                        const float4 *wq = a.Wt + hm.wt_off + ph;
-                        /* packed FP32: each lane of __ffma2_rn is a correctly rounded
-                         * fma, so (Re, Im) advance exactly as two scalar chains */
-                        float2 acc = make_float2(0.0f, 0.0f);
-#pragma unroll
-                        for (int i4 = 0; i4 < M / 4; i4++) {
-                            const float4 w = __ldg(wq + i4 * WT_STRIDE);
-                            const float2 v0 = __ldg(ap + 4 * i4), v1 = __ldg(ap + 4 * i4 + 1);
-                            const float2 v2 = __ldg(ap + 4 * i4 + 2), v3 = __ldg(ap + 4 * i4 + 3);
-                            acc = __ffma2_rn(make_float2(w.x, w.x), v0, acc);
-                            acc = __ffma2_rn(make_float2(w.y, w.y), v1, acc);
-                            acc = __ffma2_rn(make_float2(w.z, w.z), v2, acc);
-                            acc = __ffma2_rn(make_float2(w.w, w.w), v3, acc);
-                        }
-                        const float ar = acc.x, ai = acc.y;
-                        const float2 g = __ldg(a.A + hm.woff + ph);
-                        const bool inb = (b0 == bs);
-                        xr4[u] = inb ? __fsub_rn(__fmul_rn(g.x, ar), __fmul_rn(g.y, ai)) : 0.0f;
-                        xi4[u] = inb ? __fadd_rn(__fmul_rn(g.x, ai), __fmul_rn(g.y, ar)) : 0.0f;
-                        rr += R; qq += Q;
-                        if (rr >= (uint32_t)a.q) { rr -= (uint32_t)a.q; qq += 1; }
-                    }
-#pragma unroll
-                    for (int u = 0; u < 4; u++) {
-                        const float2 sc = make_float2(xr4[u] * scale, xi4[u] * scale);
-                        const __half2 hi = __float22half2_rn(sc);
-                        const float2 back = __half22float2(hi);
-                        const __half2 lo = __float22half2_rn(
-                            make_float2(__fsub_rn(sc.x, back.x), __fsub_rn(sc.y, back.y)));
-                        hw[u] = *reinterpret_cast<const uint32_t *>(&hi);
-                        lw[u] = *reinterpret_cast<const uint32_t *>(&lo);
-                    }
-                    res = rr; qint = qq;
-                } else
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const int h = 4 * hb + u + 1;
-                    float xr = 0.0f, xi = 0.0f;
-                    if (valid && ((filled >> (h - 1)) & 1ULL)) {
-                        const Harm hm = hs[h - 1];
-                        const uint32_t ph = mod_magic(t, (uint32_t)hm.P, hm.pmagic);
-                        const int base = hm.rfloor0 + (int)qint + ((int)res >= hm.carry_res ? 1 : 0);
-                        const int b0 = base + 1 - M / 2;
-                        float ar = 0.0f, ai = 0.0f;
-                        if ((unsigned)b0 <= (unsigned)(a.namps - M)) {
-                            const float2 *ap = a.amps + b0;
-                            const float4 *wq = a.Wt + hm.wt_off + ph;
-#pragma unroll
-                            for (int i4 = 0; i4 < M / 4; i4++) {
-                                const float4 w = __ldg(wq + i4 * WT_STRIDE);
-                                const float2 v0 = __ldg(ap + 4 * i4), v1 = __ldg(ap + 4 * i4 + 1);
-                                const float2 v2 = __ldg(ap + 4 * i4 + 2), v3 = __ldg(ap + 4 * i4 + 3);
-                                ar = __fmaf_rn(w.x, v0.x, ar); ai = __fmaf_rn(w.x, v0.y, ai);
-                                ar = __fmaf_rn(w.y, v1.x, ar); ai = __fmaf_rn(w.y, v1.y, ai);
-                                ar = __fmaf_rn(w.z, v2.x, ar); ai = __fmaf_rn(w.z, v2.y, ai);
-                                ar = __fmaf_rn(w.w, v3.x, ar); ai = __fmaf_rn(w.w, v3.y, ai);
-                            }
-                        }
-                        const float2 g = __ldg(a.A + hm.woff + ph);
-                        xr = __fsub_rn(__fmul_rn(g.x, ar), __fmul_rn(g.y, ai));
-                        xi = __fadd_rn(__fmul_rn(g.x, ai), __fmul_rn(g.y, ar));
-                    }
-                    const float2 sc = make_float2(xr * scale, xi * scale);
-                    const __half2 hi = __float22half2_rn(sc);
-                    const float2 back = __half22float2(hi);
-                    const __half2 lo = __float22half2_rn(
-                        make_float2(__fsub_rn(sc.x, back.x), __fsub_rn(sc.y, back.y)));
-                    hw[u] = *reinterpret_cast<const uint32_t *>(&hi);
-                    lw[u] = *reinterpret_cast<const uint32_t *>(&lo);
-                    res += R; qint += Q;   /* h -> h+1 */
-                    if (res >= (uint32_t)a.q) { res -= (uint32_t)a.q; qint += 1; }
-                }
-                /* both paths leave the state at 4hb+5; +4 more reaches block hb+2 */
-                res += r4; qint += q4;
+            uint32_t res, qint, r4, q4;
+            state_at(a, ts, 4u * par + 1u, res, qint);
+            state_at(a, ts, 4u, r4, q4);     /* step of 4 harmonics */
+            for (int hb = par; hb < HEAD; hb += 2) {
+                interp_block(a, hs, ts, hb, res, qint, scale, abuf);
+                res += r4; qint += q4;       /* 4hb+5 -> 4(hb+2)+1 */
                 if (res >= (uint32_t)a.q) { res -= (uint32_t)a.q; qint += 1; }
-                /* K block hb = columns 4hb..4hb+3 (two halves per column) */
-                tmem_st4(abuf + 4 * hb, hw[0], hw[1], hw[2], hw[3]);
-                tmem_st4(abuf + 64 + 4 * hb, lw[0], lw[1], lw[2], lw[3]);
             }
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             tc_fence_before();
@@ -484,18 +507,33 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const __grid_constant
             if (lane == 0) mbar_arrive(bar_afull + 8 * s);
         }
     } else {
-        /* --------------------- tensor cores + epilogue --------------------- */
+        /* ----- tensor cores, epilogue, and blocks HEAD..14 of the next tile ---- */
         const int e = warp - 8;
         const int quarter = e & 3, grp = e >> 2;
         const int r = quarter * 32 + lane;
+        const uint32_t tlane = (uint32_t)(quarter * 32) << 16;
         const bool leader = (warp == 8 && lane == 0);
         const uint32_t idesc = (1u << 4) | ((uint32_t)(NPAD >> 3) << 17) |
                                ((uint32_t)(CS_TILE_M >> 4) << 24);
         const uint32_t lbo_b = NPAD * 16;
         const uint32_t b_hi = smem_u32(smem + SM_B), b_lo = b_hi + BIMG;
+        /* tail blocks: group 0 has the lighter epilogue and takes more of them */
+        const int tb0 = grp == 0 ? HEAD : HEAD + G0;
+        const int tb1 = grp == 0 ? HEAD + G0 : NH / 4;
         int issued = 0, consumed = 0;
         bool ok = true;
 
+        auto tail = [&](int it, int tile) {
+            const TrialState ts = trial_state(a, tile, r);
+            const uint32_t abuf = tmem + tlane + (uint32_t)(TM_A + 128 * (it & 1));
+            uint32_t res, qint;
+            state_at(a, ts, 4u * tb0 + 1u, res, qint);
+            for (int hb = tb0; hb < tb1; hb++) interp_block(a, hs, ts, hb, res, qint, scale, abuf);
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar_afull + 8 * (it & 1));
+        };
         auto issue = [&](int it) -> bool {
             const int s = it & 1;
             if (!mbar_wait(bar_afull + 8 * s, (it >> 1) & 1)) return false;
@@ -519,18 +557,29 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const __grid_constant
             return true;
         };
 
-        if (leader && tile_begin < tile_end) {
-            ok = issue(0);
-            if (ok) issued = 1;
-            else atomicExch(a.err, 1);
+        /* tile 0: its tail blocks, then its MMAs */
+        if (tile_begin < tile_end) {
+            tail(0, tile_begin);
+            if (leader) {
+                ok = issue(0);
+                if (ok) issued = 1;
+                else atomicExch(a.err, 1);
+            }
+            __syncwarp();
         }
         int it = 0;
         for (int tile = tile_begin; tile < tile_end; tile++, it++) {
             const int s = it & 1;
-            if (leader && ok && tile + 1 < tile_end) {
-                ok = issue(it + 1);
-                if (ok) issued++;
-                else atomicExch(a.err, 1);
+            if (tile + 1 < tile_end) {
+                /* A buffer (it+1)&1 was last read by the MMA of tile it-1, whose
+                 * accumulator this group already consumed: it is free */
+                tail(it + 1, tile + 1);
+                if (leader && ok) {
+                    ok = issue(it + 1);
+                    if (ok) issued++;
+                    else atomicExch(a.err, 1);
+                }
+                __syncwarp();
             }
             bool got = mbar_wait(bar_dfull + 8 * s, (it >> 1) & 1);
             if (!epi_bar_and(got && ok)) {
