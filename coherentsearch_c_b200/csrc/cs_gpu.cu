@@ -1169,3 +1169,200 @@ CS_EXPORT int cs_b200_session_sync(GpuSession *S)
     if (!S) return -1;
     return cudaStreamSynchronize(S->st) == cudaSuccess ? 0 : -1;
 }
+
+/* ------------------------------------------------------------------ */
+/* Search without allocation (cs_b200_session_search_noalloc)          */
+/* ------------------------------------------------------------------ */
+/* Per-call scratch of the search in static device memory: amax[2], the record
+ * counter and the error flag in the first 256 bytes, then up to
+ * CS_B200_NOALLOC_MAX_RECS records.  One copy per device, so calls on the same
+ * device that overlap on the GPU (two streams, two host threads) race on it. */
+static_assert(sizeof(CsRec) == 16, "record layout");
+static_assert(sizeof(Candidate) >= sizeof(CsRec), "records are expanded in place");
+constexpr size_t NOALLOC_HDR = 256;
+constexpr size_t NOALLOC_BYTES = NOALLOC_HDR + (size_t)CS_B200_NOALLOC_MAX_RECS * sizeof(CsRec);
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static unsigned char *g_noalloc_ptr[NOALLOC_MAX_DEVICES];
+
+/* Device address of this device's scratch; looked up once per device with
+ * that device current.  The lookup can load the module, so the first call on
+ * a device belongs before any stream capture. */
+static unsigned char *noalloc_scratch(int device)
+{
+    if (device < 0 || device >= NOALLOC_MAX_DEVICES) return NULL;
+    unsigned char *p = __atomic_load_n(&g_noalloc_ptr[device], __ATOMIC_ACQUIRE);
+    if (p) return p;
+    void *addr = NULL;
+    const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+    if (e != cudaSuccess || !addr) {
+        fprintf(stderr, "Error: scratch lookup on device %d failed: %s\n", device,
+                cudaGetErrorString(e));
+        return NULL;
+    }
+    /* racing first calls store the same address */
+    __atomic_store_n(&g_noalloc_ptr[device], (unsigned char *)addr, __ATOMIC_RELEASE);
+    return (unsigned char *)addr;
+}
+
+/* (chunk, slot, j) order, as cs_sort_records; in place (heapsort), because
+ * the library qsort may take heap memory for large arrays. */
+static inline bool rec_less(const CsRec &x, const CsRec &y)
+{
+    if (x.chunk != y.chunk) return x.chunk < y.chunk;
+    if (x.slot != y.slot) return x.slot < y.slot;
+    return x.j < y.j;
+}
+
+static void rec_sift(CsRec *v, long long i, long long n)
+{
+    for (;;) {
+        long long c = 2 * i + 1;
+        if (c >= n) return;
+        if (c + 1 < n && rec_less(v[c], v[c + 1])) c++;
+        if (!rec_less(v[i], v[c])) return;
+        std::swap(v[i], v[c]);
+        i = c;
+    }
+}
+
+static void rec_heapsort(CsRec *v, long long n)
+{
+    for (long long i = n / 2 - 1; i >= 0; i--) rec_sift(v, i, n);
+    for (long long e = n - 1; e > 0; e--) {
+        std::swap(v[0], v[e]);
+        rec_sift(v, 0, e);
+    }
+}
+
+/* One record to a Candidate with the arithmetic of cs_harvest
+ * (src/cuda.cu:837-881); false if the record is not reported. */
+static bool rec_to_candidate(const GpuSession *S, const CsRec &r, double threshold,
+                             Candidate *cd)
+{
+    const double metric = (double)r.metric;
+    if (!(metric > threshold)) return false;
+    const CsSlot *s = &S->tab.slot[r.slot];
+    const double rstart = S->r_lo + (double)S->tab.chunks[r.chunk].i0 * S->lodr;
+    const double rfreq = rstart + (double)r.j * S->lodr;
+    const double kmul = (double)s->k;
+    const double rsel = kmul != 1.0 ? kmul * rfreq : rfreq;
+    if (r.slot != 0 && !(rsel < (double)S->N / 2.0)) return false;
+    cd->freq = rsel / S->T;
+    cd->metric = metric;
+    cd->r = rsel;
+    cd->nharm = s->Hk;
+    cd->ducy = NAN;
+    return true;
+}
+
+CS_EXPORT int cs_b200_session_search_noalloc(GpuSession *S, const float *d_amps,
+                                             double threshold, Candidate *out,
+                                             long long cap, long long *nout, void *stream)
+{
+    if (nout) *nout = 0;
+    if (!S || !out || !nout || cap < 0) return -1;
+    if (select_device(S->device) != cudaSuccess) return -1;
+    unsigned char *base = noalloc_scratch(S->device);
+    if (!base) return -1;
+    unsigned *amax = (unsigned *)base;               /* [2] */
+    unsigned *count = amax + 2;
+    int *err = (int *)(amax + 3);
+    CsRec *recs = (CsRec *)(base + NOALLOC_HDR);
+    cudaStream_t st = stream ? (cudaStream_t)stream : S->st;
+    const float2 *amps = d_amps ? (const float2 *)d_amps : S->d_amps;
+
+    cudaError_t e = cudaMemsetAsync(base, 0, 4 * sizeof(unsigned), st);
+    if (e == cudaSuccess && S->namps > 0) {
+        int g = (int)std::min<long long>((S->namps + 255) / 256, (long long)S->nsm * 8);
+        cs_amax_kernel<<<g, 256, 0, st>>>(amps, S->namps, amax);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && S->tab.ntiles > 0) {
+        const int grid = std::min(S->tab.ntiles, S->nsm);
+        if (S->use_ws) {
+            ws60::Args w;
+            memset(&w, 0, sizeof(w));
+            w.amps = amps;
+            w.namps = (int)S->namps;
+            w.Wt = S->d_Wt;
+            w.A = S->d_A;
+            w.harm = S->d_harm2;
+            w.chunks = S->d_chunks;
+            w.tiles = S->d_tiles;
+            w.ntiles = S->tab.ntiles;
+            w.bimg = S->d_bimg;
+            w.q = S->tab.q;
+            w.pnum = S->tab.pnum;
+            w.qmagic = magic_for(S->tab.q);
+            w.gbound = S->tab.gbound;
+            w.amax = amax;
+            w.thresh = threshold;
+            w.recs = recs;
+            w.count = count;
+            w.cap = CS_B200_NOALLOC_MAX_RECS;
+            w.err = err;
+            ws60::search_ws60<<<grid, ws60::NTHREADS, ws60::SMEM_BYTES, st>>>(w);
+        } else {
+            SearchArgs a = make_args(S, amps, threshold);
+            a.amax = amax;
+            a.recs = recs;
+            a.count = count;
+            a.cap = CS_B200_NOALLOC_MAX_RECS;
+            a.err = err;
+            const int smem = smem_bytes(S->tab);
+            if (S->tab.m == 16)
+                cs_search_kernel<16><<<grid, CS_NTHREADS, smem, st>>>(a);
+            else
+                cs_search_kernel<0><<<grid, CS_NTHREADS, smem, st>>>(a);
+        }
+        e = cudaGetLastError();
+    }
+    unsigned hdr[4] = {0, 0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hdr, base, sizeof(hdr), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "Error: B200 search failed: %s\n", cudaGetErrorString(e));
+        return -1;
+    }
+    if (hdr[3] != 0) {
+        fprintf(stderr, "Error: B200 search kernel timed out waiting for the tensor cores\n");
+        return -1;
+    }
+    const long long n = hdr[2];
+    if (n > CS_B200_NOALLOC_MAX_RECS) {
+        fprintf(stderr, "Error: %lld records above threshold %.3f exceed the %d this entry "
+                        "point holds; raise the threshold or use cs_gpu_session_run\n",
+                n, threshold, CS_B200_NOALLOC_MAX_RECS);
+        return -2;
+    }
+    if (n > cap) {
+        fprintf(stderr, "Error: %lld records above threshold need an output array of at "
+                        "least %lld candidates (given %lld)\n", n, n, cap);
+        return -3;
+    }
+    if (n == 0) return 0;
+    /* records land at the front of the caller's array and are expanded in
+     * place: Candidate i (40 B) never overlaps a record j < i (16 B) */
+    CsRec *hrec = (CsRec *)out;
+    e = cudaMemcpyAsync(hrec, recs, (size_t)n * sizeof(CsRec), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "Error: B200 search readback failed: %s\n", cudaGetErrorString(e));
+        return -1;
+    }
+    rec_heapsort(hrec, n);
+    for (long long i = n - 1; i >= 0; i--) {
+        const CsRec r = hrec[i];
+        Candidate cd;
+        memset(&cd, 0, sizeof(cd));
+        if (!rec_to_candidate(S, r, threshold, &cd)) cd.nharm = 0;   /* dropped */
+        out[i] = cd;
+    }
+    long long k = 0;
+    for (long long i = 0; i < n; i++)
+        if (out[i].nharm != 0) out[k++] = out[i];
+    *nout = k;
+    return 0;
+}

@@ -50,6 +50,39 @@ int cs_b200_session_collect(GpuSession *s, double threshold, CandidateList *out,
 
 int cs_b200_session_sync(GpuSession *s);
 
+/* ---- search without allocation --------------------------------------
+ * No reference counterpart.  cs_gpu_session_run and the enqueue/collect pair
+ * may grow the record buffer with cudaMalloc and rerun when more candidates
+ * pass the threshold than it holds, and build their result on the host heap.
+ * A caller that must not allocate once it is running cannot use them: a
+ * real-time pipeline whose latency budget has no room for the device-wide
+ * synchronisation a cudaMalloc/cudaFree implies, or a process that reserves
+ * all device memory at start-up and hands none out afterwards.
+ *
+ * This entry point runs the same kernels on a session made earlier by
+ * cs_gpu_session_create (whose tables were allocated then) and allocates
+ * nothing, on the device or the host: its per-call scratch (spectrum maximum,
+ * record counter, error flag, and up to CS_B200_NOALLOC_MAX_RECS records of
+ * 16 bytes, about 1 MiB) is a static device array, cleared at the start of
+ * each call.  The first call on a device looks up that array's address and
+ * should come before any stream capture.  The scratch is shared by every
+ * session on a device, so calls that overlap on the GPU (two streams, two
+ * host threads) race and must be serialised by the caller.
+ *
+ * d_amps: device spectrum (namps float2), or NULL for the session's buffer.
+ * out/cap: caller-owned host array for the candidates; also used as staging
+ * for the raw records, so cap must be at least the number of records above
+ * the threshold.  stream: a cudaStream_t, or NULL for the session stream; the
+ * call waits for it.  The candidates equal those of cs_gpu_session_run in
+ * content and order.  Returns 0 and *nout, -1 on a CUDA or kernel error, -2
+ * when more than CS_B200_NOALLOC_MAX_RECS records pass the threshold (nothing
+ * is returned; raise the threshold or use cs_gpu_session_run), -3 when cap is
+ * too small. */
+#define CS_B200_NOALLOC_MAX_RECS 65536
+int cs_b200_session_search_noalloc(GpuSession *s, const float *d_amps, double threshold,
+                                   Candidate *out, long long cap, long long *nout,
+                                   void *stream);
+
 #ifdef __cplusplus
 }
 #endif
