@@ -281,13 +281,8 @@ def run_b200(args):
     f_sm = (clocks.get("sm_mhz") or 1965.0) * 1e6
     simt_peak = 148 * 128 * f_sm
     simt_ach = total * SIMT_OPS_PER_TRIAL / (kms * 1e-3)
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "traffic_per_launch.json")
-    if os.path.exists(prof):
-        try:
-            traffic = json.load(open(prof)).get("bytes_per_launch")
-        except Exception:
-            traffic = None
+    kname = "search_ws60" if info.kernel == 1 else "cs_search_kernel"
+    traffic = profiled_traffic(kname, total)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -299,7 +294,7 @@ def run_b200(args):
         "gpu_launches": 2 * args.steps,
         "roofline": {"bound": "tensor", "achieved": dft_tflops, "peak": tc_peak,
                      "unit": "TFLOP/s", "frac": dft_tflops / tc_peak, "traffic": traffic,
-                     "kernel": "cs_search_kernel", "kernel_ms": kms,
+                     "kernel": kname, "kernel_ms": kms,
                      "peak_kind": f"bf16 dense, {peak_kind}",
                      "algorithmic": f"{DFT_FLOP_PER_TRIAL:.0f} DFT flop/trial x {total} trials"},
         "simt": {"achieved_lane_ops": simt_ach, "peak_lane_ops": simt_peak,
@@ -324,6 +319,27 @@ def run_b200(args):
     if pg is not None:
         pg.destroy_process_group()
     return 0
+
+
+def profiled_traffic(kernel, total):
+    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
+    summary profiles/<kernel>_n23_traffic.md, a line `bytes_per_launch: B`
+    measured on this workload (same trial count), else None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_n23_traffic.md")
+    if not os.path.exists(path):
+        return None
+    vals = {}
+    for line in open(path):
+        line = line.strip().strip("`")
+        if ":" in line:
+            k, _, v = line.partition(":")
+            vals[k.strip()] = v.strip().replace(",", "")
+    try:
+        if int(vals.get("trials", -1)) != total:
+            return None
+        return int(vals["bytes_per_launch"])
+    except (KeyError, ValueError):
+        return None
 
 
 def main():
