@@ -321,6 +321,179 @@ def run_b200(args):
     return 0
 
 
+DEDISP = {
+    "workload": "raw-data front end: 8-bit filterbank, 1024 channels, 1400 MHz centre, "
+                "300 MHz, 64 us, 2^22 spectra, DM 56.8 pulsar; 64 subbands, 500 DMs 0-199.6 "
+                "(step 0.4), SIGPROC blocks of 2400 spectra",
+    "nchan": 1024, "nsub": 64, "ndm": 500, "lodm": 0.0, "dmstep": 0.4, "nspec": 1 << 22,
+    "numout": 1 << 22,
+}
+DEDISP_METRIC = "dedispersed samples/sec/GPU"
+DEDISP_UNIT = "DM-samples/s"
+
+
+def make_filterbank_device(spec, device):
+    """The synthetic filterbank of coherentsearch_c_b200.synth.make_filterbank,
+    generated on the GPU (seeded torch generator) to keep set-up short."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(spec.seed)
+    freqs = spec.lofreq + spec.chanwid * torch.arange(spec.nchan, device=device,
+                                                      dtype=torch.float64)
+    delay = spec.dm / (0.000241 * freqs * freqs)
+    kappa = math.log(2.0) / (1.0 - math.cos(math.pi * spec.duty))
+    raw = torch.empty((spec.nspec, spec.nchan), dtype=torch.uint8, device=device)
+    chunk = 1 << 17
+    for t0 in range(0, spec.nspec, chunk):
+        n = min(chunk, spec.nspec - t0)
+        t = (t0 + torch.arange(n, device=device, dtype=torch.float64))[:, None] * spec.dt
+        phase = torch.remainder(spec.f0 * (t - delay[None, :]), 1.0)
+        pulse = torch.exp(kappa * (torch.cos(2.0 * math.pi * phase) - 1.0)).float()
+        x = spec.mean + spec.sigma * (torch.randn((n, spec.nchan), generator=g, device=device)
+                                      + spec.amp * pulse)
+        raw[t0:t0 + n] = torch.flip(torch.clamp(torch.round(x), 0, 255), dims=[1]).to(torch.uint8)
+    return raw
+
+
+def dedisp_cpu_rate(raw_host, t, seconds=10.0):
+    """The reference's dispersion.c kernels under the prepsubband block driver
+    (oracle/_ref/libdedisp_ref.so, one thread, as prepsubband runs them) on a
+    bounded stretch of the workload: all DMs over the first blocks."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import refbind as rb
+    nblk = 4 * t.blocks_per_read + 2
+    sample = raw_host[: nblk * t.spectra_per_subint]
+    reps, n_out, t0 = 0, 0, time.perf_counter()
+    while True:
+        out = rb.ref_dedisp_run(sample, t.nsub, t.idispdt, t.offsets, t.spectra_per_subint,
+                                t.blocks_per_read)
+        reps += 1
+        n_out += out.shape[0] * out.shape[1]
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    return n_out / dt, 1, (f"{reps} runs of all {t.ndm} DMs over the first {nblk} blocks "
+                           f"({sample.shape[0]} spectra, {out.shape[1]} output samples per DM)")
+
+
+def run_dedisp(args):
+    import ctypes as C
+    import torch
+    from coherentsearch_c_b200 import synth
+    from coherentsearch_c_b200.dedisp import Dedisperser, dedisp_tables
+    world, rank, local, pg = dist_setup(args)
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    W = dict(DEDISP)
+    if args.nspec_log2:
+        W["nspec"] = W["numout"] = 1 << args.nspec_log2
+        W["workload"] = W["workload"].replace("2^22 spectra", f"2^{args.nspec_log2} spectra")
+    spec = synth.config_filterbank(nspec=W["nspec"], seed=4 + rank)
+    t = dedisp_tables(W["nchan"], W["nsub"], W["ndm"], W["lodm"], W["dmstep"], spec.lofreq,
+                      spec.chanwid, spec.dt)
+    raw = make_filterbank_device(spec, dev)
+    dd = Dedisperser(t, max_spectra=spec.nspec, device=local)
+    nout = dd.output_length(spec.nspec, W["numout"])
+    stride = (nout + 3) // 4 * 4
+    out = torch.empty((t.ndm, stride), dtype=torch.float32, device=dev)
+    # a stream of our own: the legacy default stream's handle is 0, which the
+    # C ABI reads as "the plan's stream"
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+
+    def step():
+        return dd.run_device(raw.data_ptr(), spec.nspec, out.data_ptr(), stride, W["numout"],
+                             stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+    times, sb_ms, dm_ms = [], [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            a, b = dd.last_times()
+            sb_ms.append(a)
+            dm_ms.append(b)
+        torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+    ms = statistics.mean(times)
+    if pg is not None:
+        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        ms = float(tt.item())
+    samples = t.ndm * nout
+    value = world * samples / (ms * 1e-3)
+    hbm_peak, _, peak_kind = load_peaks()
+    alg_bytes = spec.nspec * t.nchan + 4.0 * samples          # raw once + output once
+    kern_ms = statistics.mean(sb_ms) + statistics.mean(dm_ms)
+    line = {
+        "metric": DEDISP_METRIC, "value": value, "unit": DEDISP_UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8->f32",
+        "data": "synthetic",
+        "config": dict(workload=W["workload"], output_per_dm=nout,
+                       blocks_per_read=t.blocks_per_read,
+                       l2="inputs larger than L2 (raw input and output both > 126 MB)",
+                       parallelism=f"replicas{world}"),
+        "gpu_launches": 2 * args.steps,
+        "roofline": {"bound": "hbm", "achieved": alg_bytes / (kern_ms * 1e-3) / 1e9,
+                     "peak": hbm_peak, "unit": "GB/s",
+                     "frac": alg_bytes / (kern_ms * 1e-3) / 1e9 / hbm_peak, "traffic": None,
+                     "kernel": "dd_subband_u8 + dd_dms_u16",
+                     "subband_ms": statistics.mean(sb_ms), "dm_ms": statistics.mean(dm_ms),
+                     "peak_kind": f"HBM copy, {peak_kind}",
+                     "algorithmic": f"{spec.nspec} x {t.nchan} B raw + {samples} x 4 B output"},
+        "clocks": clk.summary(),
+    }
+    # end to end: host (pinned) raw in, host (pinned) output back, through cs_dedisp_run
+    if not args.no_e2e:
+        h_raw = torch.empty(raw.shape, dtype=torch.uint8, pin_memory=True)
+        h_raw.copy_(raw)
+        h_out = torch.empty((t.ndm, nout), dtype=torch.float32, pin_memory=True)
+        e2e = []
+        for _ in range(max(2, args.steps // 5)):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            got = C.c_longlong(0)
+            rc = dd.lib.cs_dedisp_run(dd.plan, h_raw.data_ptr(), spec.nspec, W["numout"],
+                                      h_out.data_ptr(), nout, C.byref(got))
+            e1.record(stream)
+            e1.synchronize()
+            if rc != 0:
+                raise RuntimeError("cs_dedisp_run failed")
+            e2e.append(e0.elapsed_time(e1))
+        line["e2e"] = {"value": world * samples / (statistics.mean(e2e) * 1e-3),
+                       "unit": DEDISP_UNIT, "h2d_bytes_per_step": int(h_raw.numel()),
+                       "d2h_bytes_per_step": int(4 * samples)}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            nblk = 4 * t.blocks_per_read + 2
+            host = raw[: nblk * t.spectra_per_subint].cpu().numpy()
+            rate, cores, sample = dedisp_cpu_rate(host, t, seconds=args.cpu_seconds)
+            line["cpu_baseline"] = {"value": rate, "unit": DEDISP_UNIT, "cores": cores,
+                                    "kind": "reference", "sample": sample}
+        except Exception as exc:   # noqa: BLE001
+            line["cpu_baseline"] = {"value": None, "unit": DEDISP_UNIT, "cores": 0,
+                                    "kind": "reference", "sample": f"unavailable: {exc}"}
+    if rank == 0:
+        print(json.dumps(line))
+    dd.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
 def profiled_traffic(kernel, total):
     """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
     summary profiles/<kernel>_n23_traffic.md, a line `bytes_per_launch: B`
@@ -350,6 +523,13 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="search", choices=["search", "dedisp"],
+                    help="search: the coherent search (headline); dedisp: subband "
+                         "dedispersion of the 8-bit filterbank workload")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--nspec-log2", type=int, default=0,
+                    help="dedisp workload length 2^n spectra (default: the 2^22 workload; "
+                         "smaller sizes are for profiling captures only)")
     ap.add_argument("--nlog2", type=int, default=23,
                     help="series length 2^n (23 = the benchmark workload; smaller "
                          "sizes are for profiling captures only)")
@@ -359,6 +539,13 @@ def main():
         WORKLOAD["workload"] = WORKLOAD["workload"].replace("N=2^23", f"N=2^{args.nlog2}")
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "dedisp":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the dedispersion workload's reference arm is the cpu_baseline "
+                              "object of its own line"}))
+            return 0
+        return run_dedisp(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)

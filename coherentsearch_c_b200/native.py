@@ -151,6 +151,26 @@ def declare_gpu_api(lib: C.CDLL) -> C.CDLL:
                                                    C.c_void_p, C.c_longlong,
                                                    P(C.c_longlong), C.c_void_p]
     lib.cs_b200_session_search_noalloc.restype = C.c_int
+    IP = P(C.c_int)
+    lib.cs_dedisp_tables.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                     C.c_double, C.c_double, C.c_double, C.c_int, IP, IP, IP,
+                                     P(C.c_double)]
+    lib.cs_dedisp_tables.restype = C.c_int
+    lib.cs_dedisp_create.argtypes = [C.c_int, C.c_int, C.c_int, IP, IP, C.c_int, C.c_int,
+                                     C.c_longlong, C.c_int]
+    lib.cs_dedisp_create.restype = C.c_void_p
+    lib.cs_dedisp_output_length.argtypes = [C.c_void_p, C.c_longlong, C.c_longlong]
+    lib.cs_dedisp_output_length.restype = C.c_longlong
+    lib.cs_dedisp_run_device.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_longlong,
+                                         C.c_void_p, C.c_longlong, C.c_void_p,
+                                         P(C.c_longlong)]
+    lib.cs_dedisp_run_device.restype = C.c_int
+    lib.cs_dedisp_run.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_longlong,
+                                  C.c_void_p, C.c_longlong, P(C.c_longlong)]
+    lib.cs_dedisp_run.restype = C.c_int
+    lib.cs_dedisp_last_times.argtypes = [C.c_void_p, P(C.c_float), P(C.c_float)]
+    lib.cs_dedisp_last_times.restype = C.c_int
+    lib.cs_dedisp_free.argtypes = [C.c_void_p]
     return lib
 
 

@@ -172,3 +172,59 @@ def normalised_spectrum(x: np.ndarray, block: int = 100) -> np.ndarray:
 def amps_interleaved(S: np.ndarray) -> np.ndarray:
     """complex64[n] -> float32[2n] (re, im interleaved), the FFTFile.amps layout."""
     return np.ascontiguousarray(S, dtype=np.complex64).view(np.float32)
+
+
+# ---------------------------------------------------------------------------
+# 8-bit filterbank (raw-data front end)
+# ---------------------------------------------------------------------------
+@dataclass
+class FilterbankSpec:
+    """SIGPROC-style 8-bit filterbank: per-channel N(mean, sigma) clipped to
+    0..255 plus a dispersed von Mises pulsar.  Channels are stored highest
+    frequency first, as SIGPROC files with negative foff hold them."""
+    nchan: int = 1024
+    nspec: int = 1 << 22
+    fctr: float = 1400.0          # MHz
+    bw: float = 300.0             # MHz
+    dt: float = 64e-6
+    mean: float = 128.0
+    sigma: float = 12.0
+    dm: float = 56.8
+    f0: float = 4.1
+    duty: float = 0.04
+    amp: float = 2.0              # pulse peak per channel, in units of sigma
+    seed: int = 4
+
+    @property
+    def chanwid(self) -> float:
+        return self.bw / self.nchan
+
+    @property
+    def lofreq(self) -> float:
+        """Centre of the lowest channel (PRESTO's idata.freq,
+        third_party/presto/src/sigproc_fb.c:435-441)."""
+        return self.fctr + 0.5 * self.chanwid - 0.5 * self.bw
+
+
+def config_filterbank(nspec: int = 1 << 22, seed: int = 4) -> FilterbankSpec:
+    """1024 channels, 1400 MHz centre, 300 MHz, 64 us, DM 56.8 pulsar at
+    4.1 Hz with a 4 % duty cycle."""
+    return FilterbankSpec(nspec=nspec, seed=seed)
+
+
+def make_filterbank(spec: FilterbankSpec, chunk: int = 1 << 14) -> np.ndarray:
+    """[nspec][nchan] uint8, highest frequency first."""
+    rng = np.random.default_rng(spec.seed)
+    freqs = spec.lofreq + spec.chanwid * np.arange(spec.nchan)            # ascending
+    delay = spec.dm / (0.000241 * freqs * freqs)                           # seconds
+    kappa = von_mises_kappa(spec.duty)
+    out = np.empty((spec.nspec, spec.nchan), np.uint8)
+    for t0 in range(0, spec.nspec, chunk):
+        n = min(chunk, spec.nspec - t0)
+        t = (t0 + np.arange(n))[:, None] * spec.dt
+        phase = (spec.f0 * (t - delay[None, :])) % 1.0
+        pulse = np.exp(kappa * (np.cos(2.0 * np.pi * phase) - 1.0))
+        x = spec.mean + spec.sigma * (rng.standard_normal((n, spec.nchan)) + spec.amp * pulse)
+        np.clip(np.rint(x), 0, 255, out=x)
+        out[t0:t0 + n] = x[:, ::-1].astype(np.uint8)
+    return out

@@ -50,6 +50,51 @@ int cs_b200_session_collect(GpuSession *s, double threshold, CandidateList *out,
 
 int cs_b200_session_sync(GpuSession *s);
 
+/* ---- subband dedispersion of 8-bit filterbank data ---------------------
+ * The prepsubband stage of the reference's raw-data front end
+ * (src/prep_dedisp.c:444-466 tables, :1104-1275 block driver; PRESTO
+ * dispersion.c dedisp_subbands :218-267 and float_dedisp :322-365; the
+ * reference GPU kernels third_party/presto/src/cuda.cu:557-597, 704-768).
+ * Input: raw spectra [nspec][nchan] of unsigned 8-bit samples in SIGPROC
+ * order (highest frequency first), as the file holds them.  Output: for DM
+ * d, out[d * out_stride + t], t < the returned length, bit-identical to the
+ * reference's FP32 result for the same delays (no clipping, masking,
+ * downsampling or barycentring). */
+typedef struct CsDedisp CsDedisp;
+
+/* Delay tables as prep_dedisp.c computes them for DMs lodm + i*dmstep:
+ * idispdt[nchan] (channel delays in samples, ascending frequency),
+ * offsets[ndm*nsub] (subband offsets per DM), blocks per read and the
+ * subbanding DM.  lofreq: centre of the lowest channel (MHz); chanwid > 0. */
+int cs_dedisp_tables(int nchan, int nsub, int ndm, double lodm, double dmstep, double lofreq,
+                     double chanwid, double dt, int spectra_per_subint, int *idispdt,
+                     int *offsets, int *blocks_per_read, double *avgdm);
+
+/* Plan for up to max_spectra input spectra; NULL on invalid geometry (a
+ * delay outside the reference's limits, or sums that would not be exact). */
+CsDedisp *cs_dedisp_create(int nchan, int nsub, int ndm, const int *idispdt, const int *offsets,
+                           int spectra_per_subint, int blocks_per_read, long long max_spectra,
+                           int device);
+
+/* Output points per DM the reference writes for nspec spectra, at most
+ * numout (numout < 0: no cap). */
+long long cs_dedisp_output_length(const CsDedisp *d, long long nspec, long long numout);
+
+/* Device buffers: d_out 16-byte aligned, out_stride a multiple of 4.
+ * Enqueued on `stream` (a cudaStream_t, NULL for the plan's stream). */
+int cs_dedisp_run_device(CsDedisp *d, const uint8_t *d_raw, long long nspec, long long numout,
+                         float *d_out, long long out_stride, void *stream,
+                         long long *nout_written);
+
+/* Host buffers; copies in and out and waits. */
+int cs_dedisp_run(CsDedisp *d, const uint8_t *h_raw, long long nspec, long long numout,
+                  float *h_out, long long out_stride, long long *nout_written);
+
+/* CUDA-event times of the last run's subband and DM kernels (ms). */
+int cs_dedisp_last_times(CsDedisp *d, float *subband_ms, float *dm_ms);
+
+void cs_dedisp_free(CsDedisp *d);
+
 /* ---- search without allocation --------------------------------------
  * No reference counterpart.  cs_gpu_session_run and the enqueue/collect pair
  * may grow the record buffer with cudaMalloc and rerun when more candidates

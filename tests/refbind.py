@@ -174,3 +174,57 @@ def oracle_candidates(metrics: np.ndarray, geo, N: int, dt: float, opts, t_begin
                     continue
                 rows.append((rsel / T, float(mval), rsel, opts.nharms // k, np.nan))
     return np.array(rows, dtype=nt.CAND_DTYPE)
+
+
+# ---------------------------------------------------------------------------
+# dedispersion: the reference's dispersion.c + the restated block driver
+# ---------------------------------------------------------------------------
+_DD = None
+
+
+def have_dedisp_ref() -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "libdedisp_ref.so"))
+
+
+def dedisp_ref_lib() -> C.CDLL:
+    global _DD
+    if _DD is None:
+        lib = C.CDLL(os.path.join(REF_DIR, "libdedisp_ref.so"))
+        IP = C.POINTER(C.c_int)
+        lib.odd_tables.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                   C.c_double, C.c_double, C.c_int, C.c_int, IP, IP, IP,
+                                   C.POINTER(C.c_double)]
+        lib.odd_run.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_int, C.c_int,
+                                C.c_int, IP, IP, C.c_longlong, C.c_void_p, C.c_longlong,
+                                C.POINTER(C.c_longlong)]
+        _DD = lib
+    return _DD
+
+
+def ref_dedisp_tables(nchan, nsub, ndm, lodm, dmstep, lofreq, chanwid, dt, L=2400):
+    lib = dedisp_ref_lib()
+    idisp = np.zeros(nchan, np.int32)
+    offs = np.zeros((ndm, nsub), np.int32)
+    bpr = C.c_int(0)
+    avg = C.c_double(0)
+    IP = C.POINTER(C.c_int)
+    lib.odd_tables(nchan, nsub, ndm, lodm, dmstep, lofreq, chanwid, dt, 1, L,
+                   idisp.ctypes.data_as(IP), offs.ctypes.data_as(IP), C.byref(bpr), C.byref(avg))
+    return idisp, offs, bpr.value, avg.value
+
+
+def ref_dedisp_run(raw, nsub, idisp, offs, L, bpr, numout=-1):
+    """The reference's prepsubband output for every DM: [ndm][nout] float32."""
+    lib = dedisp_ref_lib()
+    raw = np.ascontiguousarray(raw, np.uint8)
+    nspec, nchan = raw.shape
+    ndm = offs.shape[0]
+    cap = nspec if numout < 0 else min(numout, nspec)
+    out = np.zeros((ndm, max(cap, 1)), np.float32)
+    got = C.c_longlong(0)
+    IP = C.POINTER(C.c_int)
+    idisp = np.ascontiguousarray(idisp, np.int32)
+    offs = np.ascontiguousarray(offs, np.int32)
+    lib.odd_run(raw.ctypes.data, nspec, nchan, nsub, ndm, L, bpr, idisp.ctypes.data_as(IP),
+                offs.ctypes.data_as(IP), cap, out.ctypes.data, out.shape[1], C.byref(got))
+    return out[:, :got.value]
