@@ -35,10 +35,16 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "cs_internal.h"
@@ -650,6 +656,8 @@ struct GpuSession {
     float4 *d_AC;
     ws60::Harm *d_harm2;
     ws60::Harm hh[ws60::NH];
+    /* capacities (bytes) of the buffers session_load may reuse */
+    size_t c_amps, c_rowtab, c_W, c_A, c_carry, c_chunks, c_tiles, c_bimg;
 };
 
 static cudaError_t select_device(int device)
@@ -797,20 +805,33 @@ static uint32_t magic_for(int d)
     return d >= 2 ? (uint32_t)(0x100000000ULL / (unsigned long long)d + 1ULL) : 0u;
 }
 
-CS_EXPORT GpuSession *cs_gpu_session_create(const FFTFile *ft, const SearchParams *p,
-                                            const DirectPlanSet *dplans,
-                                            const long long *cstarts, long long total,
-                                            int Nprof, long long nchunks, double r_lo,
-                                            double lodr, int device)
+/* Keep *p at least `need` bytes: reuse it when large enough, else replace it
+ * (contents are not kept). */
+static cudaError_t dev_reserve(void **p, size_t *cap, size_t need)
+{
+    if (need == 0) need = 1;
+    if (*p && *cap >= need) return cudaSuccess;
+    cudaFree(*p);
+    *p = NULL;
+    *cap = 0;
+    const cudaError_t e = cudaMalloc(p, need);
+    if (e == cudaSuccess) *cap = need;
+    return e;
+}
+
+/* Build the host tables for one geometry and bring the device copies up to
+ * date, reusing the session's device buffers where they are large enough.
+ * Returns 0, or -1 with a message.  Leaves the session unusable on failure
+ * (callers release it). */
+static int session_load(GpuSession *S, const FFTFile *ft, const SearchParams *p,
+                        const DirectPlanSet *dplans, const long long *cstarts, long long total,
+                        int Nprof, long long nchunks, double r_lo, double lodr)
 {
     char err[512] = {0};
-    GpuSession *S = (GpuSession *)calloc(1, sizeof(GpuSession));
     std::vector<uint16_t> bhi, blo;
     size_t img_halves = 0;
     int smem = 0;
-    if (!S) return NULL;
     S->p = p;
-    S->device = device;
     S->Nprof = Nprof;
     S->total = total;
     S->nchunks = nchunks;
@@ -819,64 +840,48 @@ CS_EXPORT GpuSession *cs_gpu_session_create(const FFTFile *ft, const SearchParam
     S->T = ft->T;
     S->r_lo = r_lo;
     S->lodr = lodr;
+    cs_tables_free(&S->tab);
     if (cs_tables_build(&S->tab, ft, p, dplans, cstarts, total, nchunks, r_lo, lodr,
                         err, sizeof(err)) != 0) {
         fprintf(stderr, "Error: B200 search session: %s\n", err);
-        session_release(S);
-        return NULL;
-    }
-    CK(select_device(device));
-    {
-        cudaDeviceProp prop;
-        CK(cudaGetDeviceProperties(&prop, device));
-        S->max_smem = (int)prop.sharedMemPerBlockOptin;
-        S->nsm = prop.multiProcessorCount;
+        return -1;
     }
     smem = smem_bytes(S->tab);
     if (smem > S->max_smem) {
         fprintf(stderr, "Error: B200 search kernel needs %d bytes of shared memory, device "
-                        "%d allows %d\n", smem, device, S->max_smem);
-        session_release(S);
-        return NULL;
+                        "%d allows %d\n", smem, S->device, S->max_smem);
+        return -1;
     }
-    CK(cudaStreamCreateWithFlags(&S->st, cudaStreamNonBlocking));
-    CK(cudaEventCreate(&S->ev0));
-    CK(cudaEventCreate(&S->ev1));
-    CK(cudaMalloc((void **)&S->d_amps, (size_t)(S->namps > 0 ? S->namps : 1) * sizeof(float2)));
-    CK(cudaMalloc((void **)&S->d_harm, sizeof(CsHarm) * CS_MAX_NH));
-    CK(cudaMemcpy(S->d_harm, S->tab.harm, sizeof(CsHarm) * CS_MAX_NH, cudaMemcpyHostToDevice));
-    CK(cudaMalloc((void **)&S->d_rowtab, (size_t)S->tab.nh * S->tab.q * sizeof(uint16_t)));
-    CK(cudaMemcpy(S->d_rowtab, S->tab.rowtab, (size_t)S->tab.nh * S->tab.q * sizeof(uint16_t),
+    const CsTables &t = S->tab;
+    CK(dev_reserve((void **)&S->d_amps, &S->c_amps, (size_t)S->namps * sizeof(float2)));
+    CK(cudaMemcpy(S->d_harm, t.harm, sizeof(CsHarm) * CS_MAX_NH, cudaMemcpyHostToDevice));
+    CK(dev_reserve((void **)&S->d_rowtab, &S->c_rowtab, (size_t)t.nh * t.q * sizeof(uint16_t)));
+    CK(cudaMemcpy(S->d_rowtab, t.rowtab, (size_t)t.nh * t.q * sizeof(uint16_t),
                   cudaMemcpyHostToDevice));
-    CK(cudaMalloc((void **)&S->d_W, (size_t)S->tab.nrows * S->tab.m * sizeof(float)));
-    CK(cudaMemcpy(S->d_W, S->tab.W, (size_t)S->tab.nrows * S->tab.m * sizeof(float),
-                  cudaMemcpyHostToDevice));
-    CK(cudaMalloc((void **)&S->d_A, (size_t)S->tab.nrows * sizeof(float2)));
-    CK(cudaMemcpy(S->d_A, S->tab.A, (size_t)S->tab.nrows * sizeof(float2), cudaMemcpyHostToDevice));
-    CK(cudaMalloc((void **)&S->d_carry, (size_t)S->tab.nrows));
-    CK(cudaMemcpy(S->d_carry, S->tab.carry, (size_t)S->tab.nrows, cudaMemcpyHostToDevice));
-    CK(cudaMalloc((void **)&S->d_chunks, (size_t)(nchunks > 0 ? nchunks : 1) * sizeof(CsChunk)));
+    CK(dev_reserve((void **)&S->d_W, &S->c_W, (size_t)t.nrows * t.m * sizeof(float)));
+    CK(cudaMemcpy(S->d_W, t.W, (size_t)t.nrows * t.m * sizeof(float), cudaMemcpyHostToDevice));
+    CK(dev_reserve((void **)&S->d_A, &S->c_A, (size_t)t.nrows * sizeof(float2)));
+    CK(cudaMemcpy(S->d_A, t.A, (size_t)t.nrows * sizeof(float2), cudaMemcpyHostToDevice));
+    CK(dev_reserve((void **)&S->d_carry, &S->c_carry, (size_t)t.nrows));
+    CK(cudaMemcpy(S->d_carry, t.carry, (size_t)t.nrows, cudaMemcpyHostToDevice));
+    CK(dev_reserve((void **)&S->d_chunks, &S->c_chunks, (size_t)nchunks * sizeof(CsChunk)));
     if (nchunks > 0)
-        CK(cudaMemcpy(S->d_chunks, S->tab.chunks, (size_t)nchunks * sizeof(CsChunk),
+        CK(cudaMemcpy(S->d_chunks, t.chunks, (size_t)nchunks * sizeof(CsChunk),
                       cudaMemcpyHostToDevice));
-    CK(cudaMalloc((void **)&S->d_tiles, (size_t)(S->tab.ntiles > 0 ? S->tab.ntiles : 1) * 3 * sizeof(int)));
-    if (S->tab.ntiles > 0)
-        CK(cudaMemcpy(S->d_tiles, S->tab.tiles, (size_t)S->tab.ntiles * 3 * sizeof(int),
+    CK(dev_reserve((void **)&S->d_tiles, &S->c_tiles, (size_t)t.ntiles * 3 * sizeof(int)));
+    if (t.ntiles > 0)
+        CK(cudaMemcpy(S->d_tiles, t.tiles, (size_t)t.ntiles * 3 * sizeof(int),
                       cudaMemcpyHostToDevice));
-    img_halves = (size_t)S->tab.npad * S->tab.kpad;
+    img_halves = (size_t)t.npad * t.kpad;
     bhi.resize(img_halves);
     blo.resize(img_halves);
     cs_tables_dft_images(&S->tab, bhi.data(), blo.data());
     S->bbytes = (int)(img_halves * 2);
-    CK(cudaMalloc((void **)&S->d_bimg, (size_t)2 * S->bbytes));
+    CK(dev_reserve((void **)&S->d_bimg, &S->c_bimg, (size_t)2 * S->bbytes));
     CK(cudaMemcpy(S->d_bimg, bhi.data(), (size_t)S->bbytes, cudaMemcpyHostToDevice));
     CK(cudaMemcpy((char *)S->d_bimg + S->bbytes, blo.data(), (size_t)S->bbytes,
                   cudaMemcpyHostToDevice));
-    CK(cudaMalloc((void **)&S->d_amax, 2 * sizeof(unsigned)));
-    CK(cudaMalloc((void **)&S->d_count, sizeof(unsigned)));
-    CK(cudaMalloc((void **)&S->d_err, sizeof(int)));
-    CK(cudaMallocHost((void **)&S->h_count, 4 * sizeof(unsigned)));
-    S->use_ws = ws60_applies(S->tab, total) && S->namps < 2147483000LL &&
+    S->use_ws = ws60_applies(t, total) && S->namps < 2147483000LL &&
                 ws60::SMEM_BYTES <= S->max_smem;
     if (S->use_ws) {
         /* weights: harmonic h, tap quad i4, phase p at float4
@@ -884,37 +889,88 @@ CS_EXPORT GpuSession *cs_gpu_session_create(const FFTFile *ft, const SearchParam
         const size_t nq = (size_t)ws60::NH * 4 * ws60::WT_STRIDE;
         std::vector<float> wfix(nq * 4, 0.0f);
         for (int h = 0; h < ws60::NH; h++) {
-            S->hh[h].rfloor0 = (int)S->tab.harm[h].rfloor0;
-            S->hh[h].P = S->tab.harm[h].P;
-            S->hh[h].woff = S->tab.harm[h].woff;
+            S->hh[h].rfloor0 = (int)t.harm[h].rfloor0;
+            S->hh[h].P = t.harm[h].P;
+            S->hh[h].woff = t.harm[h].woff;
             S->hh[h].wt_off = h * 4 * ws60::WT_STRIDE;
-            S->hh[h].pmagic = magic_for(S->tab.harm[h].P);
-            S->hh[h].carry_res = S->tab.carry_res[h];
-            const int P = S->tab.harm[h].P, off = S->tab.harm[h].woff;
+            S->hh[h].pmagic = magic_for(t.harm[h].P);
+            S->hh[h].carry_res = t.carry_res[h];
+            const int P = t.harm[h].P, off = t.harm[h].woff;
             for (int ph = 0; ph < P; ph++)
                 for (int i = 0; i < ws60::M; i++)
                     wfix[4 * ((size_t)h * 4 * ws60::WT_STRIDE + (i / 4) * ws60::WT_STRIDE + ph) + (i & 3)] =
-                        S->tab.W[(size_t)(off + ph) * S->tab.m + i];
+                        t.W[(size_t)(off + ph) * t.m + i];
         }
-        CK(cudaMalloc((void **)&S->d_harm2, sizeof(ws60::Harm) * ws60::NH));
+        if (!S->d_harm2) CK(cudaMalloc((void **)&S->d_harm2, sizeof(ws60::Harm) * ws60::NH));
         CK(cudaMemcpy(S->d_harm2, S->hh, sizeof(ws60::Harm) * ws60::NH, cudaMemcpyHostToDevice));
-        CK(cudaMalloc((void **)&S->d_Wt, nq * sizeof(float4)));
+        if (!S->d_Wt) CK(cudaMalloc((void **)&S->d_Wt, nq * sizeof(float4)));
         CK(cudaMemcpy(S->d_Wt, wfix.data(), nq * sizeof(float4), cudaMemcpyHostToDevice));
         CK(cudaFuncSetAttribute(ws60::search_ws60, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 ws60::SMEM_BYTES));
     }
     {
         /* Start with room for 1 in 16 trials per slot; grown on overflow. */
-        long long want = (total * S->tab.nslot) / 16 + 4096;
+        long long want = (total * t.nslot) / 16 + 4096;
         if (want > (long long)0x7fffffff) want = 0x7fffffff;
-        if (grow_records(S, (unsigned)want) != 0) { session_release(S); return NULL; }
+        if (!S->d_recs || S->cap < (unsigned)want)
+            if (grow_records(S, (unsigned)want) != 0) return -1;
     }
     CK(cudaFuncSetAttribute(cs_search_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     CK(cudaFuncSetAttribute(cs_search_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return 0;
+fail:
+    return -1;
+}
+
+/* Device bytes a session holds for its current geometry. */
+static size_t session_bytes(const GpuSession *S)
+{
+    return S->c_amps + S->c_rowtab + S->c_W + S->c_A + S->c_carry + S->c_chunks + S->c_tiles +
+           S->c_bimg + (size_t)S->cap * sizeof(CsRec) + sizeof(CsHarm) * CS_MAX_NH +
+           (S->d_Wt ? (size_t)ws60::NH * 4 * ws60::WT_STRIDE * sizeof(float4) : 0);
+}
+
+/* A session on `device` with its streams, events and fixed-size buffers,
+ * but no geometry yet; NULL on failure. */
+static GpuSession *session_new(int device)
+{
+    GpuSession *S = (GpuSession *)calloc(1, sizeof(GpuSession));
+    if (!S) return NULL;
+    S->device = device;
+    CK(select_device(device));
+    {
+        cudaDeviceProp prop;
+        CK(cudaGetDeviceProperties(&prop, device));
+        S->max_smem = (int)prop.sharedMemPerBlockOptin;
+        S->nsm = prop.multiProcessorCount;
+    }
+    CK(cudaStreamCreateWithFlags(&S->st, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&S->ev0));
+    CK(cudaEventCreate(&S->ev1));
+    CK(cudaMalloc((void **)&S->d_harm, sizeof(CsHarm) * CS_MAX_NH));
+    CK(cudaMalloc((void **)&S->d_amax, 2 * sizeof(unsigned)));
+    CK(cudaMalloc((void **)&S->d_count, sizeof(unsigned)));
+    CK(cudaMalloc((void **)&S->d_err, sizeof(int)));
+    CK(cudaMallocHost((void **)&S->h_count, 4 * sizeof(unsigned)));
     return S;
 fail:
     session_release(S);
     return NULL;
+}
+
+CS_EXPORT GpuSession *cs_gpu_session_create(const FFTFile *ft, const SearchParams *p,
+                                            const DirectPlanSet *dplans,
+                                            const long long *cstarts, long long total,
+                                            int Nprof, long long nchunks, double r_lo,
+                                            double lodr, int device)
+{
+    GpuSession *S = session_new(device);
+    if (!S) return NULL;
+    if (session_load(S, ft, p, dplans, cstarts, total, Nprof, nchunks, r_lo, lodr) != 0) {
+        session_release(S);
+        return NULL;
+    }
+    return S;
 }
 
 CS_EXPORT int cs_gpu_session_matches(const GpuSession *S, const FFTFile *ft,
@@ -1365,4 +1421,308 @@ CS_EXPORT int cs_b200_session_search_noalloc(GpuSession *S, const float *d_amps,
         if (out[i].nharm != 0) out[k++] = out[i];
     *nout = k;
     return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* Batched search of many spectra (cs_gpu_batch_*)                     */
+/* ------------------------------------------------------------------ */
+/* One request: a spectrum and its search.  The spectrum stays in the
+ * caller's memory until the request is waited for. */
+struct BatchReq {
+    long long id;
+    FFTFile ft;
+    SearchParams p;
+    double lofreq, hifreq, threshold;
+    int lobin, blocksize;
+    CandidateList out;
+    int status;                      /* 0 ok, -1 error */
+    bool done;
+    std::chrono::steady_clock::time_point t_submit, t_start, t_end;
+};
+
+/* What a slot's session was last loaded for. */
+struct BatchKey {
+    long long N, namps, total;
+    double T, r_lo, lodr;
+    int Nprof;
+    SearchParams p;
+};
+
+struct BatchSlot {
+    GpuSession *S = nullptr;
+    BatchKey key;
+    bool keyed = false;
+    bool busy = false;
+    size_t bytes = 0;
+};
+
+struct CsBatch {
+    int device = 0;
+    size_t budget = 0;               /* device bytes all slots may hold; 0: no limit */
+    std::vector<BatchSlot> slots;
+    std::vector<std::thread> workers;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done, cv_mem;
+    std::deque<BatchReq *> queue;
+    std::unordered_map<long long, BatchReq *> reqs;
+    long long next_id = 0;
+    bool stop = false;
+};
+
+/* Geometry of a request, as search_file derives it (src/search.c:1247-1262). */
+static bool batch_geometry(const BatchReq *r, double *r_lo, double *lodr, long long *total,
+                           int *Nprof)
+{
+    *lodr = r->p.hidr / (double)r->p.nharms;
+    *r_lo = r->lobin != 100 ? (double)r->lobin : r->lofreq * r->ft.T;
+    const double r_hi = r->hifreq * r->ft.T;
+    *total = (long long)floor((r_hi - *r_lo) / *lodr) + 1;
+    *Nprof = r->blocksize > 0 ? r->blocksize : 65536;
+    return *total > 0;
+}
+
+/* Device bytes a request's session needs (spectrum, records, tiles, chunk
+ * and interpolation tables), before any reuse. */
+static size_t batch_footprint(const BatchReq *r, long long total, int Nprof)
+{
+    const long long recs = (total * (r->p.ndecim + 1)) / 16 + 4096;
+    const long long nchunks = total / std::max(1, Nprof) + 2 * r->p.nharms + 2;
+    return (size_t)r->ft.namps * sizeof(float2) + (size_t)recs * sizeof(CsRec) +
+           (size_t)(total / CS_TILE_M + nchunks + 1) * 3 * sizeof(int) +
+           (size_t)nchunks * sizeof(CsChunk) + ((size_t)4 << 20);
+}
+
+/* Admit slot k for a request needing `need` bytes: wait (lock held by the
+ * caller through `lk`) until the slots' device memory fits the budget,
+ * releasing the sessions of idle slots, and this slot's own, when that makes
+ * room.  Returns false if the request can never fit. */
+static bool batch_admit(CsBatch *B, int k, size_t need, std::unique_lock<std::mutex> &lk)
+{
+    if (B->budget == 0) return true;
+    if (need > B->budget) return false;
+    for (;;) {
+        size_t others = 0;
+        for (size_t j = 0; j < B->slots.size(); j++)
+            if ((int)j != k) others += B->slots[j].bytes;
+        BatchSlot &me = B->slots[k];
+        if (others + std::max(me.bytes, need) <= B->budget) return true;
+        /* make room: this slot's own buffers first, then idle slots' */
+        bool freed = false;
+        if (me.S && me.bytes > need) {
+            session_release(me.S);
+            me.S = nullptr;
+            me.keyed = false;
+            me.bytes = 0;
+            freed = true;
+        }
+        for (size_t j = 0; j < B->slots.size() && !freed; j++) {
+            BatchSlot &o = B->slots[j];
+            if ((int)j != k && !o.busy && o.S) {
+                session_release(o.S);
+                o.S = nullptr;
+                o.keyed = false;
+                o.bytes = 0;
+                freed = true;
+            }
+        }
+        if (!freed) B->cv_mem.wait(lk);
+    }
+}
+
+static void batch_run_one(CsBatch *B, int k, BatchReq *r)
+{
+    BatchSlot &slot = B->slots[k];
+    candlist_init(&r->out);
+    r->status = -1;
+    double r_lo, lodr;
+    long long total;
+    int Nprof;
+    if (!batch_geometry(r, &r_lo, &lodr, &total, &Nprof)) {
+        r->status = 0;                               /* empty band: no trials */
+        return;
+    }
+    BatchKey key;
+    memset(&key, 0, sizeof(key));
+    key.N = r->ft.N;
+    key.namps = r->ft.namps;
+    key.total = total;
+    key.T = r->ft.T;
+    key.r_lo = r_lo;
+    key.lodr = lodr;
+    key.Nprof = Nprof;
+    key.p = r->p;
+    GpuSession *S = slot.S;
+    if (!S) {
+        S = session_new(B->device);
+        if (!S) return;
+        slot.S = S;
+        slot.keyed = false;
+    }
+    if (!slot.keyed || memcmp(&key, &slot.key, sizeof(key)) != 0) {
+        DirectPlanSet plans;
+        memset(&plans, 0, sizeof(plans));
+        long long *cstarts = NULL, nchunks = 0;
+        slot.keyed = false;
+        if (direct_plans_build(&plans, &r->p, r_lo) != 0) return;
+        const int rc = chunk_starts(&plans, &r->ft, &r->p, total, Nprof, &cstarts, &nchunks);
+        const int lrc = rc == 0 ? session_load(S, &r->ft, &r->p, &plans, cstarts, total, Nprof,
+                                               nchunks, r_lo, lodr)
+                                : -1;
+        free(cstarts);
+        direct_plans_free(&plans);
+        if (lrc != 0) return;
+        slot.key = key;
+        slot.keyed = true;
+    }
+    S->p = &r->p;
+    if (S->namps > 0 &&
+        cudaMemcpyAsync(S->d_amps, r->ft.amps, (size_t)S->namps * sizeof(float2),
+                        cudaMemcpyHostToDevice, S->st) != cudaSuccess) {
+        fprintf(stderr, "Error: batch spectrum upload failed\n");
+        return;
+    }
+    for (int attempt = 0; attempt < 2; attempt++) {
+        if (enqueue_search(S, S->d_amps, r->threshold, false) != cudaSuccess) {
+            fprintf(stderr, "Error: batch search launch failed\n");
+            candlist_free(&r->out);
+            return;
+        }
+        int rerun = 0;
+        if (collect(S, r->threshold, &r->out, &rerun) != 0) {
+            candlist_free(&r->out);
+            return;
+        }
+        if (!rerun) break;
+    }
+    r->status = 0;
+}
+
+static void batch_worker(CsBatch *B, int k)
+{
+    select_device(B->device);
+    std::unique_lock<std::mutex> lk(B->mu);
+    for (;;) {
+        B->cv_work.wait(lk, [&] { return B->stop || !B->queue.empty(); });
+        if (B->stop && B->queue.empty()) break;
+        BatchReq *r = B->queue.front();
+        B->queue.pop_front();
+        double r_lo, lodr;
+        long long total;
+        int Nprof;
+        const size_t need = batch_geometry(r, &r_lo, &lodr, &total, &Nprof)
+                                ? batch_footprint(r, total, Nprof) : 0;
+        r->t_start = std::chrono::steady_clock::now();
+        if (!batch_admit(B, k, need, lk)) {
+            fprintf(stderr, "Error: batch request %lld needs about %zu device bytes, more than "
+                            "the budget of %zu\n", r->id, need, B->budget);
+            candlist_init(&r->out);
+            r->status = -1;
+        } else {
+            B->slots[k].busy = true;
+            /* reserve the room while the slot grows into it */
+            B->slots[k].bytes = std::max(B->slots[k].bytes, need);
+            lk.unlock();
+            batch_run_one(B, k, r);
+            lk.lock();
+            BatchSlot &slot = B->slots[k];
+            slot.busy = false;
+            slot.bytes = slot.S ? session_bytes(slot.S) : 0;
+        }
+        r->t_end = std::chrono::steady_clock::now();
+        r->done = true;
+        B->cv_done.notify_all();
+        B->cv_mem.notify_all();
+    }
+}
+
+CS_EXPORT CsBatch *cs_gpu_batch_create(int device, int nslots, size_t mem_budget)
+{
+    if (nslots < 1 || nslots > 16) {
+        fprintf(stderr, "Error: cs_gpu_batch_create: 1 to 16 slots\n");
+        return NULL;
+    }
+    char msg[256];
+    if (cs_gpu_available(device, msg, sizeof(msg)) != 1) {
+        fprintf(stderr, "Error: cs_gpu_batch_create: %s\n", msg);
+        return NULL;
+    }
+    CsBatch *B = new CsBatch();
+    B->device = device;
+    B->budget = mem_budget;
+    B->slots.resize(nslots);
+    for (int k = 0; k < nslots; k++) B->workers.emplace_back(batch_worker, B, k);
+    return B;
+}
+
+CS_EXPORT long long cs_gpu_batch_submit(CsBatch *B, const FFTFile *ft, const SearchParams *p,
+                                        double lofreq, double hifreq, int lobin, int blocksize,
+                                        double threshold)
+{
+    if (!B || !ft || !p || (ft->namps > 0 && !ft->amps)) return -1;
+    BatchReq *r = new BatchReq();
+    r->ft = *ft;
+    r->p = *p;
+    r->lofreq = lofreq;
+    r->hifreq = hifreq;
+    r->lobin = lobin;
+    r->blocksize = blocksize;
+    r->threshold = threshold;
+    r->done = false;
+    r->status = -1;
+    candlist_init(&r->out);
+    r->t_submit = std::chrono::steady_clock::now();
+    std::lock_guard<std::mutex> g(B->mu);
+    r->id = B->next_id++;
+    B->reqs[r->id] = r;
+    B->queue.push_back(r);
+    B->cv_work.notify_one();
+    return r->id;
+}
+
+CS_EXPORT int cs_gpu_batch_wait(CsBatch *B, long long id, CandidateList *out, double *queued_ms,
+                                double *run_ms)
+{
+    if (out) candlist_init(out);
+    if (!B) return -1;
+    std::unique_lock<std::mutex> lk(B->mu);
+    auto it = B->reqs.find(id);
+    if (it == B->reqs.end()) return -1;
+    BatchReq *r = it->second;
+    B->cv_done.wait(lk, [&] { return r->done; });
+    B->reqs.erase(it);
+    lk.unlock();
+    const int status = r->status;
+    if (out) out->v = r->out.v, out->n = r->out.n, out->cap = r->out.cap;
+    else candlist_free(&r->out);
+    using ms = std::chrono::duration<double, std::milli>;
+    if (queued_ms) *queued_ms = ms(r->t_start - r->t_submit).count();
+    if (run_ms) *run_ms = ms(r->t_end - r->t_start).count();
+    delete r;
+    return status;
+}
+
+CS_EXPORT int cs_gpu_batch_pending(CsBatch *B)
+{
+    if (!B) return -1;
+    std::lock_guard<std::mutex> g(B->mu);
+    return (int)B->reqs.size();
+}
+
+CS_EXPORT void cs_gpu_batch_free(CsBatch *B)
+{
+    if (!B) return;
+    {
+        std::lock_guard<std::mutex> g(B->mu);
+        B->stop = true;
+    }
+    B->cv_work.notify_all();
+    for (auto &t : B->workers) t.join();
+    select_device(B->device);
+    for (auto &sl : B->slots)
+        if (sl.S) session_release(sl.S);
+    for (auto &kv : B->reqs) {
+        candlist_free(&kv.second->out);
+        delete kv.second;
+    }
+    delete B;
 }

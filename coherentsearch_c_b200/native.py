@@ -151,6 +151,17 @@ def declare_gpu_api(lib: C.CDLL) -> C.CDLL:
                                                    C.c_void_p, C.c_longlong,
                                                    P(C.c_longlong), C.c_void_p]
     lib.cs_b200_session_search_noalloc.restype = C.c_int
+    lib.cs_gpu_batch_create.argtypes = [C.c_int, C.c_int, C.c_size_t]
+    lib.cs_gpu_batch_create.restype = C.c_void_p
+    lib.cs_gpu_batch_submit.argtypes = [C.c_void_p, P(FFTFile), P(SearchParams), C.c_double,
+                                        C.c_double, C.c_int, C.c_int, C.c_double]
+    lib.cs_gpu_batch_submit.restype = C.c_longlong
+    lib.cs_gpu_batch_wait.argtypes = [C.c_void_p, C.c_longlong, P(CandidateList),
+                                      P(C.c_double), P(C.c_double)]
+    lib.cs_gpu_batch_wait.restype = C.c_int
+    lib.cs_gpu_batch_pending.argtypes = [C.c_void_p]
+    lib.cs_gpu_batch_pending.restype = C.c_int
+    lib.cs_gpu_batch_free.argtypes = [C.c_void_p]
     IP = P(C.c_int)
     lib.cs_dedisp_tables.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                      C.c_double, C.c_double, C.c_double, C.c_int, IP, IP, IP,

@@ -50,6 +50,43 @@ int cs_b200_session_collect(GpuSession *s, double threshold, CandidateList *out,
 
 int cs_b200_session_sync(GpuSession *s);
 
+/* ---- batched search of many spectra -------------------------------------
+ * No reference counterpart: the reference searches one file per call
+ * (src/search.c:1388-1406) and rebuilds its GPU session whenever the file
+ * length changes.  Here requests (one spectrum each, any length and search
+ * parameters) run on a pool of `nslots` slots, each a session with its own
+ * host thread and CUDA stream.  One request's table building and upload
+ * overlap another's kernel, and a slot's device buffers are reused across
+ * lengths.  A slot takes a request only while the device memory that all
+ * slots hold stays within `mem_budget` bytes (0: no limit); idle slots give
+ * their buffers back when another slot needs the room. */
+typedef struct CsBatch CsBatch;
+
+CsBatch *cs_gpu_batch_create(int device, int nslots, size_t mem_budget);
+
+/* Queue the search of one spectrum over [lofreq, hifreq] Hz (lobin != 100
+ * overrides the low edge, blocksize 0 means 65536), as search_file would run
+ * it.  ft and *p are copied; ft->amps (host memory; pinned memory uploads at
+ * full speed) must stay valid until the request is waited for.  Returns the
+ * request id, or -1. */
+long long cs_gpu_batch_submit(CsBatch *b, const FFTFile *ft, const SearchParams *p,
+                              double lofreq, double hifreq, int lobin, int blocksize,
+                              double threshold);
+
+/* Wait for one request.  *out receives its raw candidates exactly as
+ * cs_gpu_session_run returns them (owned by the caller); queued_ms and run_ms
+ * (optional) the time it waited for a slot and the time the slot spent on
+ * it.  Returns 0, or -1 (unknown id, or the search failed). */
+int cs_gpu_batch_wait(CsBatch *b, long long id, CandidateList *out, double *queued_ms,
+                      double *run_ms);
+
+/* Requests submitted and not yet waited for. */
+int cs_gpu_batch_pending(CsBatch *b);
+
+/* Finishes the queued requests, then frees everything (results not waited
+ * for are dropped). */
+void cs_gpu_batch_free(CsBatch *b);
+
 /* ---- subband dedispersion of 8-bit filterbank data ---------------------
  * The prepsubband stage of the reference's raw-data front end
  * (src/prep_dedisp.c:444-466 tables, :1104-1275 block driver; PRESTO
