@@ -30,6 +30,8 @@ import subprocess
 import sys
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -494,6 +496,185 @@ def run_dedisp(args):
     return 0
 
 
+def spectrum_device(N, dt, seed, pulsars, device):
+    """A normalised spectrum as synth.normalised_spectrum builds it (white
+    noise + von Mises pulse trains, PRESTO-packed forward FFT, unit power by
+    block medians of 100 bins), computed on the GPU and returned in pinned
+    host memory as interleaved float32 (a spectrum read from a file)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    x = torch.randn(N, generator=g, device=device, dtype=torch.float64)
+    t = torch.arange(N, device=device, dtype=torch.float64) * dt
+    for p in pulsars:
+        kappa = math.log(2.0) / (1.0 - math.cos(math.pi * p.duty))
+        s = torch.exp(kappa * (torch.cos(2.0 * math.pi * torch.remainder(t * p.f0 + p.phase0, 1.0))
+                               - 1.0))
+        s = s - s.mean()
+        x = x + (p.snr / torch.sqrt(torch.dot(s, s))) * s
+    X = torch.fft.rfft(x)
+    n2 = N // 2
+    S = X[:n2].clone()
+    pw = (S.real ** 2 + S.imag ** 2)
+    nb = (n2 - 1) // 100
+    scale = torch.ones(n2, device=device, dtype=torch.float64)
+    if nb > 0:
+        med = torch.quantile(pw[1:1 + nb * 100].reshape(nb, 100), 0.5, dim=1) / math.log(2.0)
+        med[med <= 0] = 1.0
+        scale[1:1 + nb * 100] = torch.repeat_interleave(1.0 / torch.sqrt(med), 100)
+        scale[1 + nb * 100:] = 1.0 / torch.sqrt(med[-1])
+    S = (S * scale).to(torch.complex64)
+    S[0] = 1.0 + 0.0j
+    out = torch.empty(2 * n2, dtype=torch.float32, pin_memory=True)
+    out.copy_(torch.view_as_real(S).reshape(-1))
+    return out
+
+
+def _same_cands(a, b):
+    return a.size == b.size and all(np.array_equal(a[f], b[f]) for f in ("r", "metric", "nharm"))
+
+
+def run_sweep(args):
+    """Config 3: 256 files of uneven length searched plain (a session per
+    file, the reference's single-file GPU form) and batched (cs_gpu_batch)."""
+    import torch
+    from coherentsearch_c_b200 import synth
+    from coherentsearch_c_b200.batch import Batch
+    from coherentsearch_c_b200.search import Options, Session
+    torch.cuda.set_device(0)
+    specs = synth.config_dm_sweep(n_files=args.files)
+    dt = specs[0].dt
+    spectra = [spectrum_device(sp.N, dt, sp.seed, sp.pulsars, "cuda:0").numpy() for sp in specs]
+    nh_list = [60, 32]
+    lines = {}
+    for nh in nh_list:
+        opts = Options(nharms=nh, blocksize=65536, threshold=8.0)
+        trials = sum(int(opts.geometry(sp.N, dt)[2]) for sp in specs)
+
+        def plain():
+            out = []
+            for sp, a in zip(specs, spectra):
+                ses = Session(sp.N, dt, opts)
+                out.append(ses.run_raw(a))
+                ses.close()
+            return out
+
+        def batched():
+            with Batch(nslots=args.slots) as b:
+                ids = [b.submit(a, sp.N, dt, opts) for sp, a in zip(specs, spectra)]
+                return [b.wait(i)[0] for i in ids]
+
+        for _ in range(args.warmup):      # warm: modules, allocator, page cache
+            with Batch(nslots=args.slots) as b:
+                for i in [b.submit(a, sp.N, dt, opts) for sp, a in zip(specs[:4], spectra[:4])]:
+                    b.wait(i)
+        stream = torch.cuda.current_stream()
+        res = {}
+        for name, fn in (("plain", plain), ("batched", batched)):
+            ts = []
+            for _ in range(max(1, min(args.steps, 2))):
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                out = fn()
+                e1.record(stream)
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            res[name] = (statistics.mean(ts), out)
+        equal = all(_same_cands(x, y) for x, y in zip(res["plain"][1], res["batched"][1]))
+        lines[nh] = {"trials": trials, "plain_ms": res["plain"][0], "batched_ms": res["batched"][0],
+                     "plain_trials_per_s": trials / (res["plain"][0] * 1e-3),
+                     "batched_trials_per_s": trials / (res["batched"][0] * 1e-3),
+                     "batched_vs_plain": res["plain"][0] / res["batched"][0],
+                     "equal_candidates": bool(equal),
+                     "candidates": int(sum(o.size for o in res["batched"][1]))}
+    h2d = int(sum(a.nbytes for a in spectra))
+    main = lines[60]
+    line = {
+        "metric": METRIC, "value": main["batched_trials_per_s"], "unit": UNIT, "n_gpus": 1,
+        "steps": max(1, min(args.steps, 2)), "warmup": args.warmup,
+        "ms_per_step": main["batched_ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"batched DM sweep: {args.files} spectra, lengths log-uniform "
+                               "2^21-2^23 (dt 64 us), pulsar 11.2 Hz peaking mid-list; "
+                               f"{args.slots} batch slots",
+                   "inputs": "pinned host memory, uploaded inside the timed region",
+                   "l2": "inputs larger than L2 in aggregate", "parallelism": "replicas1"},
+        "e2e": {"value": main["batched_trials_per_s"], "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 16 * main["candidates"]},
+        "gpu_launches": 2 * args.files,
+        "sweep": {str(k): v for k, v in lines.items()},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_serve(args):
+    """Config 5: a Poisson stream of search requests served by the request
+    loop (continuous batching) and by the plain per-request form."""
+    import torch
+    from coherentsearch_c_b200 import synth
+    from coherentsearch_c_b200.search import Options
+    from coherentsearch_c_b200.serve import (PlainServer, Request, SearchServer,
+                                             log_uniform_lengths, poisson_arrivals, run_stream)
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(7)
+    dt = 64e-6
+    npool = args.pool
+    lengths = log_uniform_lengths(npool, 1 << 20, 1 << 24, seed=11)
+    pool = []
+    for i, N in enumerate(lengths):
+        pulsars = []
+        if rng.random() < 0.3:
+            pulsars = [synth.Pulsar(float(math.exp(rng.uniform(math.log(0.5), math.log(100.0)))),
+                                    float(rng.uniform(0.02, 0.10)), float(rng.uniform(8, 30)))]
+        pool.append((N, spectrum_device(N, dt, 5000 + i, pulsars, "cuda:0").numpy()))
+    reqs = []
+    for i in range(args.requests):
+        N, a = pool[int(rng.integers(npool))]
+        nh = int(rng.choice([16, 32, 60]))
+        reqs.append(Request(a, N, dt, Options(nharms=nh, blocksize=65536, threshold=8.0)))
+    arrivals = poisson_arrivals(len(reqs), rate=args.rate, seed=3)
+    # warm both forms on a few requests
+    with SearchServer(nslots=args.slots) as srv:
+        run_stream(srv, reqs[:6], np.zeros(6))
+    with PlainServer() as pl:
+        run_stream(pl, reqs[:3], np.zeros(3))
+    with ClockSampler(0) as clk:
+        with SearchServer(nslots=args.slots, mem_budget=args.mem_budget_gb << 30) as srv:
+            served = run_stream(srv, reqs, arrivals)
+    with PlainServer() as pl:
+        plain = run_stream(pl, reqs, arrivals)
+    equal = all(_same_cands(x, y) for x, y in zip(served["results"], plain["results"]))
+    trials = served["trials"]
+    line = {
+        "metric": METRIC, "value": served["trials_per_s"], "unit": UNIT, "n_gpus": 1,
+        "steps": 1, "warmup": 1, "ms_per_step": 1e3 * served["wall_s"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"serving stream: {len(reqs)} requests, Poisson {args.rate}/s, "
+                               "N log-uniform 2^20-2^24, nharms in {16, 32, 60}, 30% with a "
+                               f"pulsar (spectra from a pool of {npool}); {args.slots} slots, "
+                               f"{args.mem_budget_gb} GB budget",
+                   "inputs": "pinned host memory, uploaded per request",
+                   "parallelism": "replicas1"},
+        "latency_ms": {"p50": served["p50_ms"], "p99": served["p99_ms"], "mean": served["mean_ms"]},
+        "plain": {"trials_per_s": plain["trials_per_s"], "p50_ms": plain["p50_ms"],
+                  "p99_ms": plain["p99_ms"], "mean_ms": plain["mean_ms"],
+                  "wall_s": plain["wall_s"]},
+        "served_vs_plain": served["trials_per_s"] / plain["trials_per_s"],
+        "equal_candidates": bool(equal), "trials": trials,
+        "e2e": {"value": served["trials_per_s"], "unit": UNIT,
+                "h2d_bytes_per_step": int(sum(r.amps.nbytes for r in reqs)),
+                "d2h_bytes_per_step": int(16 * sum(x.size for x in served["results"]))},
+        "gpu_launches": 2 * len(reqs),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def profiled_traffic(kernel, total):
     """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
     summary profiles/<kernel>_n23_traffic.md, a line `bytes_per_launch: B`
@@ -523,9 +704,18 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="search", choices=["search", "dedisp"],
+    ap.add_argument("--workload", default="search",
+                    choices=["search", "dedisp", "sweep", "serve"],
                     help="search: the coherent search (headline); dedisp: subband "
-                         "dedispersion of the 8-bit filterbank workload")
+                         "dedispersion of the 8-bit filterbank workload; sweep: batched "
+                         "search of a list of uneven-length files; serve: a Poisson "
+                         "stream of requests through the request loop")
+    ap.add_argument("--files", type=int, default=256, help="sweep: number of files")
+    ap.add_argument("--slots", type=int, default=3, help="sweep/serve: batch slots")
+    ap.add_argument("--requests", type=int, default=800, help="serve: requests")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
+    ap.add_argument("--pool", type=int, default=48, help="serve: distinct spectra")
+    ap.add_argument("--mem-budget-gb", type=int, default=24, help="serve: device budget")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--nspec-log2", type=int, default=0,
                     help="dedisp workload length 2^n spectra (default: the 2^22 workload; "
@@ -539,6 +729,12 @@ def main():
         WORKLOAD["workload"] = WORKLOAD["workload"].replace("N=2^23", f"N=2^{args.nlog2}")
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload in ("sweep", "serve"):
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "this workload's baseline is its plain-form object"}))
+            return 0
+        return run_sweep(args) if args.workload == "sweep" else run_serve(args)
     if args.workload == "dedisp":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable":

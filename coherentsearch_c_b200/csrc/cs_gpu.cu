@@ -819,6 +819,17 @@ static cudaError_t dev_reserve(void **p, size_t *cap, size_t need)
     return e;
 }
 
+/* Raise a kernel's dynamic shared-memory cap to what the device allows
+ * beside the kernel's static shared memory. */
+static cudaError_t set_smem_cap(const void *fn, int max_optin)
+{
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                max_optin - (int)fa.sharedSizeBytes);
+}
+
 /* Build the host tables for one geometry and bring the device copies up to
  * date, reusing the session's device buffers where they are large enough.
  * Returns 0, or -1 with a message.  Leaves the session unusable on failure
@@ -915,8 +926,11 @@ static int session_load(GpuSession *S, const FFTFile *ft, const SearchParams *p,
         if (!S->d_recs || S->cap < (unsigned)want)
             if (grow_records(S, (unsigned)want) != 0) return -1;
     }
-    CK(cudaFuncSetAttribute(cs_search_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CK(cudaFuncSetAttribute(cs_search_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    /* the cap is per kernel, not per session: sessions of other geometries may
+     * launch concurrently (batch slots), so it is set to the device limit,
+     * never lowered to this geometry's need */
+    CK(set_smem_cap((const void *)cs_search_kernel<16>, S->max_smem));
+    CK(set_smem_cap((const void *)cs_search_kernel<0>, S->max_smem));
     return 0;
 fail:
     return -1;
