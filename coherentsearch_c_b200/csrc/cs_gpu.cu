@@ -654,8 +654,8 @@ struct GpuSession {
     int use_ws;
     float4 *d_Wt;
     float4 *d_AC;
-    ws60::Harm *d_harm2;
-    ws60::Harm hh[ws60::NH];
+    wsk::Harm *d_harm2;
+    wsk::Harm hh[wsk::MAX_NH];
     /* capacities (bytes) of the buffers session_load may reuse */
     size_t c_amps, c_rowtab, c_W, c_A, c_carry, c_chunks, c_tiles, c_bimg;
 };
@@ -771,23 +771,25 @@ static int grow_records(GpuSession *S, unsigned cap)
     return 0;
 }
 
-/* The warp-specialised kernel is compiled for the reference's default
- * search at nharms = 60: m = 16, decimations 1..6 (all folds), ladder widths
- * {1,2,3,4,6} for k = 1 and {2,3,4,6} above, and 32-bit trial positions. */
-static int ws60_applies(const CsTables &t, long long total)
+/* The warp-specialised kernels are compiled for the reference's default
+ * search at nharms = 60, 32 and 16: m = 16, decimations 1..6 and the slot
+ * layouts and ladder widths of wsk::kCfgDescs, with 32-bit trial positions.
+ * Returns the nharms of the matching configuration, or 0. */
+static int ws_config(const CsTables &t, long long total)
 {
     if (getenv("CS_B200_GENERIC_KERNEL")) return 0;
-    if (t.nh != ws60::NH || t.m != ws60::M || t.nslot != 6) return 0;
-    if (t.kpad != ws60::KPAD || t.npad != ws60::NPAD) return 0;
-    static const int wb[5] = {1, 2, 3, 4, 6}, wd[4] = {2, 3, 4, 6};
+    if (t.m != wsk::M || t.nslot != 6) return 0;
+    const wsk::CfgDesc *cd = NULL;
+    for (const wsk::CfgDesc &c : wsk::kCfgDescs)
+        if (c.nh == t.nh) cd = &c;
+    if (!cd || t.kpad != cd->kpad || t.npad != cd->npad) return 0;
     for (int s = 0; s < 6; s++) {
         const CsSlot &sl = t.slot[s];
-        if (sl.k != s + 1) return 0;
-        if (s > 0 && !sl.fold) return 0;
-        const int *w = s == 0 ? wb : wd;
-        const int nw = s == 0 ? 5 : 4;
-        if (sl.nw != nw) return 0;
-        for (int i = 0; i < nw; i++) if (sl.widths[i] != w[i]) return 0;
+        const wsk::SlotDesc &d = cd->slot[s];
+        if (sl.k != d.k || sl.nk != d.nk || (sl.fold != 0) != (d.fold != 0) || sl.nw != d.nw)
+            return 0;
+        if (s > 0 && !d.fold && sl.col0 != d.col0) return 0;
+        for (int i = 0; i < d.nw; i++) if (sl.widths[i] != d.w[i]) return 0;
     }
     /* 32-bit positions: t < 2^31 and rfloor0 + floor(t*h*pnum/q) + 1 < 2^31 */
     const double tmax = (double)total + CS_TILE_M;
@@ -796,8 +798,33 @@ static int ws60_applies(const CsTables &t, long long total)
     for (int h = 0; h < t.nh; h++) rmax = std::max(rmax, (double)t.harm[h].rfloor0);
     if (rmax + tmax * t.nh * (double)t.pnum / (double)t.q + 64 >= 2147483647.0) return 0;
     if ((double)t.q * 5.0 * t.q >= 4294967295.0) return 0;
-    for (int h = 0; h < t.nh; h++) if (t.harm[h].P > ws60::WT_STRIDE) return 0;
-    return 1;
+    for (int h = 0; h < t.nh; h++) if (t.harm[h].P > wsk::WT_STRIDE) return 0;
+    return t.nh;
+}
+
+static int ws_smem(int nh)
+{
+    return nh == 60 ? wsk::smem_bytes<wsk::Cfg60>()
+         : nh == 32 ? wsk::smem_bytes<wsk::Cfg32>()
+                    : wsk::smem_bytes<wsk::Cfg16>();
+}
+
+static cudaError_t ws_prepare(int nh)
+{
+    const void *fn = nh == 60 ? (const void *)wsk::search_ws<wsk::Cfg60>
+                   : nh == 32 ? (const void *)wsk::search_ws<wsk::Cfg32>
+                              : (const void *)wsk::search_ws<wsk::Cfg16>;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, ws_smem(nh));
+}
+
+static void ws_launch(int nh, int grid, cudaStream_t st, const wsk::Args &w)
+{
+    if (nh == 60)
+        wsk::search_ws<wsk::Cfg60><<<grid, wsk::NTHREADS, ws_smem(60), st>>>(w);
+    else if (nh == 32)
+        wsk::search_ws<wsk::Cfg32><<<grid, wsk::NTHREADS, ws_smem(32), st>>>(w);
+    else
+        wsk::search_ws<wsk::Cfg16><<<grid, wsk::NTHREADS, ws_smem(16), st>>>(w);
 }
 
 static uint32_t magic_for(int d)
@@ -892,32 +919,32 @@ static int session_load(GpuSession *S, const FFTFile *ft, const SearchParams *p,
     CK(cudaMemcpy(S->d_bimg, bhi.data(), (size_t)S->bbytes, cudaMemcpyHostToDevice));
     CK(cudaMemcpy((char *)S->d_bimg + S->bbytes, blo.data(), (size_t)S->bbytes,
                   cudaMemcpyHostToDevice));
-    S->use_ws = ws60_applies(t, total) && S->namps < 2147483000LL &&
-                ws60::SMEM_BYTES <= S->max_smem;
+    S->use_ws = ws_config(t, total);
+    if (S->use_ws && (S->namps >= 2147483000LL || ws_smem(S->use_ws) > S->max_smem))
+        S->use_ws = 0;
     if (S->use_ws) {
         /* weights: harmonic h, tap quad i4, phase p at float4
-         * h*4*WT_STRIDE + i4*WT_STRIDE + p */
-        const size_t nq = (size_t)ws60::NH * 4 * ws60::WT_STRIDE;
-        std::vector<float> wfix(nq * 4, 0.0f);
-        for (int h = 0; h < ws60::NH; h++) {
+         * h*4*WT_STRIDE + i4*WT_STRIDE + p (room for the largest nharms) */
+        const size_t nq = (size_t)wsk::MAX_NH * 4 * wsk::WT_STRIDE;
+        std::vector<float> wfix((size_t)t.nh * 4 * wsk::WT_STRIDE * 4, 0.0f);
+        for (int h = 0; h < t.nh; h++) {
             S->hh[h].rfloor0 = (int)t.harm[h].rfloor0;
             S->hh[h].P = t.harm[h].P;
             S->hh[h].woff = t.harm[h].woff;
-            S->hh[h].wt_off = h * 4 * ws60::WT_STRIDE;
+            S->hh[h].wt_off = h * 4 * wsk::WT_STRIDE;
             S->hh[h].pmagic = magic_for(t.harm[h].P);
             S->hh[h].carry_res = t.carry_res[h];
             const int P = t.harm[h].P, off = t.harm[h].woff;
             for (int ph = 0; ph < P; ph++)
-                for (int i = 0; i < ws60::M; i++)
-                    wfix[4 * ((size_t)h * 4 * ws60::WT_STRIDE + (i / 4) * ws60::WT_STRIDE + ph) + (i & 3)] =
+                for (int i = 0; i < wsk::M; i++)
+                    wfix[4 * ((size_t)h * 4 * wsk::WT_STRIDE + (i / 4) * wsk::WT_STRIDE + ph) + (i & 3)] =
                         t.W[(size_t)(off + ph) * t.m + i];
         }
-        if (!S->d_harm2) CK(cudaMalloc((void **)&S->d_harm2, sizeof(ws60::Harm) * ws60::NH));
-        CK(cudaMemcpy(S->d_harm2, S->hh, sizeof(ws60::Harm) * ws60::NH, cudaMemcpyHostToDevice));
+        if (!S->d_harm2) CK(cudaMalloc((void **)&S->d_harm2, sizeof(wsk::Harm) * wsk::MAX_NH));
+        CK(cudaMemcpy(S->d_harm2, S->hh, sizeof(wsk::Harm) * t.nh, cudaMemcpyHostToDevice));
         if (!S->d_Wt) CK(cudaMalloc((void **)&S->d_Wt, nq * sizeof(float4)));
-        CK(cudaMemcpy(S->d_Wt, wfix.data(), nq * sizeof(float4), cudaMemcpyHostToDevice));
-        CK(cudaFuncSetAttribute(ws60::search_ws60, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                ws60::SMEM_BYTES));
+        CK(cudaMemcpy(S->d_Wt, wfix.data(), wfix.size() * sizeof(float), cudaMemcpyHostToDevice));
+        CK(ws_prepare(S->use_ws));
     }
     {
         /* Start with room for 1 in 16 trials per slot; grown on overflow. */
@@ -941,7 +968,7 @@ static size_t session_bytes(const GpuSession *S)
 {
     return S->c_amps + S->c_rowtab + S->c_W + S->c_A + S->c_carry + S->c_chunks + S->c_tiles +
            S->c_bimg + (size_t)S->cap * sizeof(CsRec) + sizeof(CsHarm) * CS_MAX_NH +
-           (S->d_Wt ? (size_t)ws60::NH * 4 * ws60::WT_STRIDE * sizeof(float4) : 0);
+           (S->d_Wt ? (size_t)wsk::MAX_NH * 4 * wsk::WT_STRIDE * sizeof(float4) : 0);
 }
 
 /* A session on `device` with its streams, events and fixed-size buffers,
@@ -1048,7 +1075,7 @@ static cudaError_t enqueue_search(GpuSession *S, const float2 *d_amps, double th
     }
     if (S->tab.ntiles <= 0) return cudaGetLastError();
     if (S->use_ws) {
-        ws60::Args w;
+        wsk::Args w;
         memset(&w, 0, sizeof(w));
         w.amps = d_amps;
         w.namps = (int)S->namps;
@@ -1071,7 +1098,7 @@ static cudaError_t enqueue_search(GpuSession *S, const float2 *d_amps, double th
         w.err = S->d_err;
         const int grid = std::min(S->tab.ntiles, S->nsm);
         if (timed) cudaEventRecord(S->ev0, S->st);
-        ws60::search_ws60<<<grid, ws60::NTHREADS, ws60::SMEM_BYTES, S->st>>>(w);
+        ws_launch(S->use_ws, grid, S->st, w);
         if (timed) cudaEventRecord(S->ev1, S->st);
         return cudaGetLastError();
     }
@@ -1196,7 +1223,7 @@ CS_EXPORT int cs_b200_session_info(const GpuSession *S, CsB200Info *info)
     info->nslot = S->tab.nslot;
     info->npad = S->tab.npad;
     info->kpad = S->tab.kpad;
-    info->smem_bytes = S->use_ws ? ws60::SMEM_BYTES : smem_bytes(S->tab);
+    info->smem_bytes = S->use_ws ? ws_smem(S->use_ws) : smem_bytes(S->tab);
     info->grid = std::min(S->tab.ntiles, S->nsm);
     info->kernel = S->use_ws ? 1 : 0;
     info->total = S->total;
@@ -1352,7 +1379,7 @@ CS_EXPORT int cs_b200_session_search_noalloc(GpuSession *S, const float *d_amps,
     if (e == cudaSuccess && S->tab.ntiles > 0) {
         const int grid = std::min(S->tab.ntiles, S->nsm);
         if (S->use_ws) {
-            ws60::Args w;
+            wsk::Args w;
             memset(&w, 0, sizeof(w));
             w.amps = amps;
             w.namps = (int)S->namps;
@@ -1373,7 +1400,7 @@ CS_EXPORT int cs_b200_session_search_noalloc(GpuSession *S, const float *d_amps,
             w.count = count;
             w.cap = CS_B200_NOALLOC_MAX_RECS;
             w.err = err;
-            ws60::search_ws60<<<grid, ws60::NTHREADS, ws60::SMEM_BYTES, st>>>(w);
+            ws_launch(S->use_ws, grid, st, w);
         } else {
             SearchArgs a = make_args(S, amps, threshold);
             a.amax = amax;

@@ -1,6 +1,8 @@
 /*
- * Warp-specialised search kernel for the default decimation ladder
- * (nharms = 60, m = 16, k = 1..6, ladder widths {1,2,3,4,6} / {2,3,4,6}).
+ * Warp-specialised search kernels for the default decimation ladder
+ * (m = 16, k = 1..6) at nharms = 60, 32 and 16: one template, one
+ * configuration per harmonic count (the profile columns, the width banks of
+ * each decimation and how the epilogue splits them; see Cfg60/Cfg32/Cfg16).
  *
  * One persistent CTA per SM, 16 warps:
  *   warps 0-7   interpolation of harmonic blocks 0..HEAD-1 of tile i into
@@ -16,36 +18,44 @@
  * the bin count and widths known at compile time, the cyclic prefix, the
  * sliding window differences P[i] - P[i-w] and the k-fold sums all unroll
  * into straight-line FP32 code in the reference's expression order.
+ * Decimations k that do not divide nharms have profiles of their own (their
+ * harmonic sub-stack through its own DFT columns, src/search.c:402-407),
+ * scanned the same way without a fold.
  */
 #pragma once
 
-namespace ws60 {
+namespace wsk {
 
-constexpr int NH = 60;
-constexpr int NB = 2 * NH;          /* 120 bins */
 constexpr int M = 16;               /* interpolation taps */
 constexpr int NTHREADS = 512;
-constexpr int KPAD = 128;
-constexpr int NPAD = 128;
-constexpr int BIMG = NPAD * KPAD * 2;        /* one fp16 B image */
-/* tensor memory (512 columns): accumulators D0, D1 at columns 0 and 128;
- * operands A0, A1 (hi: K/2 = 64 columns, then lo: 64 columns) at 256, 384 */
+constexpr int MAX_NH = 60;
+/* tensor memory (512 columns): accumulators D0, D1 at columns 0 and 128
+ * (N <= 128); operands A0, A1 (hi: K/2 columns, then lo: K/2 columns) from
+ * column 256 */
 constexpr int TMEM_COLS = 512;
-constexpr int TM_D = 0, TM_A = 256;
+constexpr int TM_D = 0, TM_A = 256, D_STRIDE = 128;
 /* float4 stride between the tap quads of one harmonic in the weight table
- * (the largest phase-cycle length the kernel accepts, so the four loads of
+ * (the largest phase-cycle length the kernels accept, so the four loads of
  * a row use immediate offsets) */
 constexpr int WT_STRIDE = 128;
 
-
-/* ladder widths: {1,2,3,4,6} at k = 1, {2,3,4,6} above (src/boxcar.c:100-133) */
-struct WBase {
-    static constexpr int n = 5, wmax = 6;
-    static __host__ __device__ constexpr int w(int a) { return a < 4 ? a + 1 : 6; }
-};
-struct WDec {
-    static constexpr int n = 4, wmax = 6;
-    static __host__ __device__ constexpr int w(int a) { return a < 3 ? a + 2 : 6; }
+/* a bank of boxcar widths (src/boxcar.c:78-133), ascending */
+template <int... W>
+struct Widths {
+    static constexpr int n = sizeof...(W);
+    static __host__ __device__ constexpr int w(int a)
+    {
+        constexpr int v[] = {W...};
+        return v[a];
+    }
+    static __host__ __device__ constexpr int max_w()
+    {
+        constexpr int v[] = {W...};
+        int m = 0;
+        for (int i = 0; i < n; i++) m = v[i] > m ? v[i] : m;
+        return m;
+    }
+    static constexpr int wmax = max_w();
 };
 
 /* per-harmonic header in shared memory */
@@ -78,14 +88,6 @@ struct Args {
     unsigned cap;
     int *err;
 };
-
-/* shared memory: B hi/lo | barriers | tmem slot | harmonic headers; the
- * rest of the SM's 256 KB stays L1 for the weight and spectrum reads */
-constexpr int SM_B = 0;
-constexpr int SM_BAR = 2 * BIMG;
-constexpr int SM_TM = SM_BAR + 64;
-constexpr int SM_HARM = SM_TM + 16;
-constexpr int SMEM_BYTES = SM_HARM + NH * (int)sizeof(Harm);
 
 template <class WS>
 struct Scan {
@@ -173,12 +175,25 @@ static __device__ __forceinline__ float scan_finish(const Scan<WS> &s, const flo
     return best;
 }
 
-/* Full-resolution profile: columns 0..NB-1 of the accumulator row. */
+/* The cyclic wrap: the first wmax profile elements again as steps
+ * NK+1 .. NK+wmax, in pairs and a single last step when wmax is odd. */
+template <int NK, class WS>
+static __device__ __forceinline__ void scan_wrap(Scan<WS> &s, const float *first)
+{
+#pragma unroll
+    for (int u = 0; u + 1 < WS::wmax; u += 2) scan_push2<NK, WS>(s, first[u], first[u + 1], NK + 1 + u);
+    if (WS::wmax % 2) scan_push<NK, WS>(s, first[WS::wmax - 1], NK + WS::wmax);
+}
+
+/* Full-resolution profile: columns 0..NB-1 of the accumulator row, streamed
+ * 32 columns at a time. */
+template <int NB, class WS>
 static __device__ __forceinline__ float base_metric(uint32_t trow, const float *invsw)
 {
-    Scan<WBase> s;
+    static_assert(NB % 2 == 0 && NB >= WS::wmax, "profile shape");
+    Scan<WS> s;
     scan_init(s);
-    float first[WBase::wmax];
+    float first[WS::wmax];
 #pragma unroll
     for (int c = 0; c < (NB + 31) / 32; c++) {
         float v[32];
@@ -187,25 +202,23 @@ static __device__ __forceinline__ float base_metric(uint32_t trow, const float *
         for (int u = 0; u < 32; u += 2) {
             const int i = 32 * c + u + 1;
             if (i + 1 <= NB) {
-                if (i - 1 < WBase::wmax) first[i - 1] = v[u];
-                if (i < WBase::wmax) first[i] = v[u + 1];
-                scan_push2<NB, WBase>(s, v[u], v[u + 1], i);
+                if (i - 1 < WS::wmax) first[i - 1] = v[u];
+                if (i < WS::wmax) first[i] = v[u + 1];
+                scan_push2<NB, WS>(s, v[u], v[u + 1], i);
             }
         }
     }
-    static_assert(NB % 2 == 0 && WBase::wmax % 2 == 0, "pairwise scan");
-#pragma unroll
-    for (int u = 0; u < WBase::wmax; u += 2)
-        scan_push2<NB, WBase>(s, first[u], first[u + 1], NB + 1 + u);
+    scan_wrap<NB>(s, first);
     return scan_finish<NB>(s, invsw);
 }
 
-/* k-fold average of the full profile (src/search.c:298-331): r[j] is the
- * left-to-right FP32 sum of x[j + q*NK], times (1/k), then the boxcar. */
-template <int K>
+/* k-fold average of the full NB-bin profile (src/search.c:298-331): r[j] is
+ * the left-to-right FP32 sum of x[j + q*NK], times (1/k), then the boxcar. */
+template <int NB, int K, class WS>
 static __device__ __forceinline__ float fold_metric(uint32_t trow, const float *invsw)
 {
     constexpr int NK = NB / K;
+    static_assert(NK * K == NB && NK % 2 == 0 && NK >= WS::wmax, "fold shape");
     float r[NK];
 #pragma unroll
     for (int c = 0; c < (NB + 15) / 16; c++) {
@@ -221,15 +234,32 @@ static __device__ __forceinline__ float fold_metric(uint32_t trow, const float *
         }
     }
     const float invk = 1.0f / (float)K;
-    Scan<WDec> s;
+    Scan<WS> s;
     scan_init(s);
 #pragma unroll
     for (int j = 0; j < NK; j++) r[j] = __fmul_rn(r[j], invk);
-    static_assert(NK % 2 == 0 && WDec::wmax % 2 == 0, "pairwise scan");
 #pragma unroll
-    for (int j = 0; j < NK; j += 2) scan_push2<NK, WDec>(s, r[j], r[j + 1], j + 1);
+    for (int j = 0; j < NK; j += 2) scan_push2<NK, WS>(s, r[j], r[j + 1], j + 1);
+    scan_wrap<NK>(s, r);
+    return scan_finish<NK>(s, invsw);
+}
+
+/* A decimation that does not fold: its own NK-bin profile in accumulator
+ * columns COL0 .. COL0+NK-1 (the loads may read past it, inside the
+ * accumulator's 128 columns). */
+template <int COL0, int NK, class WS>
+static __device__ __forceinline__ float own_metric(uint32_t trow, const float *invsw)
+{
+    static_assert(NK % 2 == 0 && NK >= WS::wmax && COL0 + 16 * ((NK + 15) / 16) <= D_STRIDE,
+                  "profile shape");
+    float r[16 * ((NK + 15) / 16)];
 #pragma unroll
-    for (int u = 0; u < WDec::wmax; u += 2) scan_push2<NK, WDec>(s, r[u], r[u + 1], NK + 1 + u);
+    for (int c = 0; c < (NK + 15) / 16; c++) tmem_ld16(trow + COL0 + 16 * c, r + 16 * c);
+    Scan<WS> s;
+    scan_init(s);
+#pragma unroll
+    for (int j = 0; j < NK; j += 2) scan_push2<NK, WS>(s, r[j], r[j + 1], j + 1);
+    scan_wrap<NK>(s, r);
     return scan_finish<NK>(s, invsw);
 }
 
@@ -301,8 +331,6 @@ static __device__ __forceinline__ uint32_t mod_magic(uint32_t t, uint32_t P, uin
 }
 
 
-constexpr int HEAD = 12;            /* blocks 0..HEAD-1: interpolation warps */
-constexpr int G0 = 2;               /* blocks HEAD..HEAD+G0-1: epilogue group 0; rest group 1 */
 
 struct TrialState {
     uint32_t t, Q, R;               /* trial index, t*pnum = Q*q + R */
@@ -342,6 +370,7 @@ static __device__ __forceinline__ void state_at(const Args &a, const TrialState 
  * arithmetic) and store them, split into fp16 hi/lo, as K block hb of the
  * A operand in tensor memory.  (res, qint) enter at h = 4hb+1 and leave at
  * h = 4hb+5. */
+template <int AHALF>
 static __device__ __forceinline__ void interp_block(const Args &a, const Harm *hs,
                                                     const TrialState &ts, int hb,
                                                     uint32_t &res, uint32_t &qint,
@@ -427,13 +456,128 @@ static __device__ __forceinline__ void interp_block(const Args &a, const Harm *h
         hw[u] = *reinterpret_cast<const uint32_t *>(&hi);
         lw[u] = *reinterpret_cast<const uint32_t *>(&lo);
     }
-    /* K block hb = columns 4hb..4hb+3 (two halves per column) */
+    /* K block hb = columns 4hb..4hb+3 (two halves per column); lo K/2 columns on */
     tmem_st4(abuf + 4 * hb, hw[0], hw[1], hw[2], hw[3]);
-    tmem_st4(abuf + 64 + 4 * hb, lw[0], lw[1], lw[2], lw[3]);
+    tmem_st4(abuf + AHALF + 4 * hb, lw[0], lw[1], lw[2], lw[3]);
 }
 
-__global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const __grid_constant__ Args a)
+/* Threshold one metric of slot S of this row (warp-aggregated compaction). */
+template <int S>
+static __device__ __forceinline__ void post(const Args &a, const CsChunk &ch, float m, bool valid,
+                                            int ci, int j, int lane)
 {
+    emit(a, valid && j < ch.nvalid[S] && (double)m > a.thresh, ci, S, j, m, lane);
+}
+
+using W5 = Widths<1, 2, 3, 4, 6>;
+using W4 = Widths<2, 3, 4, 6>;
+using W3 = Widths<2, 3, 4>;
+using W2 = Widths<2, 3>;
+
+/* Per harmonic count: MMA shape (N = profile columns, K = 2*nharms padded),
+ * the split of harmonic blocks between the roles (blocks 0..HEAD-1 on the
+ * interpolation warps, HEAD..HEAD+G0-1 on epilogue group 0, the rest on
+ * group 1) and the epilogue.  Slots are in the host tables' order: k = 1,
+ * then k = 2..6; a k that does not divide nharms has its own profile columns
+ * after the 2*nharms of the base profile (cs_tables.c), at the offsets and
+ * with the width banks (src/boxcar.c:100-133) written out below.  Each
+ * group's epilogue work is balanced against its share of the blocks. */
+struct Cfg60 {
+    static constexpr int NH = 60, NPAD = 128, KPAD = 128, HEAD = 12, G0 = 2;
+    static __device__ __forceinline__ void epilogue(int grp, uint32_t trow, const CsChunk &ch,
+                                                    const Args &a, bool valid, int ci, int j,
+                                                    int lane, float inv)
+    {
+        if (grp == 0) {
+            post<0>(a, ch, base_metric<120, W5>(trow, ch.invsw[0]) * inv, valid, ci, j, lane);
+            post<5>(a, ch, fold_metric<120, 6, W4>(trow, ch.invsw[5]) * inv, valid, ci, j, lane);
+        } else {
+            post<1>(a, ch, fold_metric<120, 2, W4>(trow, ch.invsw[1]) * inv, valid, ci, j, lane);
+            post<2>(a, ch, fold_metric<120, 3, W4>(trow, ch.invsw[2]) * inv, valid, ci, j, lane);
+            post<3>(a, ch, fold_metric<120, 4, W4>(trow, ch.invsw[3]) * inv, valid, ci, j, lane);
+            post<4>(a, ch, fold_metric<120, 5, W4>(trow, ch.invsw[4]) * inv, valid, ci, j, lane);
+        }
+    }
+};
+
+struct Cfg32 {
+    static constexpr int NH = 32, NPAD = 112, KPAD = 64, HEAD = 6, G0 = 1;
+    static __device__ __forceinline__ void epilogue(int grp, uint32_t trow, const CsChunk &ch,
+                                                    const Args &a, bool valid, int ci, int j,
+                                                    int lane, float inv)
+    {
+        if (grp == 0) {
+            post<0>(a, ch, base_metric<64, W5>(trow, ch.invsw[0]) * inv, valid, ci, j, lane);
+            post<4>(a, ch, own_metric<84, 12, W2>(trow, ch.invsw[4]) * inv, valid, ci, j, lane);
+            post<5>(a, ch, own_metric<96, 10, W2>(trow, ch.invsw[5]) * inv, valid, ci, j, lane);
+        } else {
+            post<1>(a, ch, fold_metric<64, 2, W4>(trow, ch.invsw[1]) * inv, valid, ci, j, lane);
+            post<2>(a, ch, own_metric<64, 20, W4>(trow, ch.invsw[2]) * inv, valid, ci, j, lane);
+            post<3>(a, ch, fold_metric<64, 4, W3>(trow, ch.invsw[3]) * inv, valid, ci, j, lane);
+        }
+    }
+};
+
+struct Cfg16 {
+    static constexpr int NH = 16, NPAD = 64, KPAD = 32, HEAD = 3, G0 = 1;
+    static __device__ __forceinline__ void epilogue(int grp, uint32_t trow, const CsChunk &ch,
+                                                    const Args &a, bool valid, int ci, int j,
+                                                    int lane, float inv)
+    {
+        if (grp == 0) {
+            post<0>(a, ch, base_metric<32, W5>(trow, ch.invsw[0]) * inv, valid, ci, j, lane);
+            post<5>(a, ch, own_metric<48, 4, Widths<1>>(trow, ch.invsw[5]) * inv, valid, ci, j,
+                    lane);
+        } else {
+            post<1>(a, ch, fold_metric<32, 2, W3>(trow, ch.invsw[1]) * inv, valid, ci, j, lane);
+            post<2>(a, ch, own_metric<32, 10, W2>(trow, ch.invsw[2]) * inv, valid, ci, j, lane);
+            post<3>(a, ch, fold_metric<32, 4, Widths<2>>(trow, ch.invsw[3]) * inv, valid, ci, j,
+                    lane);
+            post<4>(a, ch, own_metric<42, 6, Widths<1>>(trow, ch.invsw[4]) * inv, valid, ci, j,
+                    lane);
+        }
+    }
+};
+
+/* The same layouts for the host's check that a session's tables are the
+ * ones a configuration was compiled for. */
+struct SlotDesc {
+    int k, nk, fold, col0, nw, w[6];
+};
+struct CfgDesc {
+    int nh, npad, kpad;
+    SlotDesc slot[6];
+};
+static const CfgDesc kCfgDescs[3] = {
+    {60, 128, 128, {{1, 120, 0, 0, 5, {1, 2, 3, 4, 6}}, {2, 60, 1, -1, 4, {2, 3, 4, 6}},
+                    {3, 40, 1, -1, 4, {2, 3, 4, 6}}, {4, 30, 1, -1, 4, {2, 3, 4, 6}},
+                    {5, 24, 1, -1, 4, {2, 3, 4, 6}}, {6, 20, 1, -1, 4, {2, 3, 4, 6}}}},
+    {32, 112, 64, {{1, 64, 0, 0, 5, {1, 2, 3, 4, 6}}, {2, 32, 1, -1, 4, {2, 3, 4, 6}},
+                   {3, 20, 0, 64, 4, {2, 3, 4, 6}}, {4, 16, 1, -1, 3, {2, 3, 4}},
+                   {5, 12, 0, 84, 2, {2, 3}}, {6, 10, 0, 96, 2, {2, 3}}}},
+    {16, 64, 32, {{1, 32, 0, 0, 5, {1, 2, 3, 4, 6}}, {2, 16, 1, -1, 3, {2, 3, 4}},
+                  {3, 10, 0, 32, 2, {2, 3}}, {4, 8, 1, -1, 1, {2}},
+                  {5, 6, 0, 42, 1, {1}}, {6, 4, 0, 48, 1, {1}}}},
+};
+
+template <class C>
+__host__ __device__ constexpr int smem_bytes()
+{
+    return 2 * C::NPAD * C::KPAD * 2 + 64 + 16 + C::NH * (int)sizeof(Harm);
+}
+
+template <class C>
+__global__ void __launch_bounds__(NTHREADS, 1) search_ws(const __grid_constant__ Args a)
+{
+    constexpr int NH = C::NH, NPAD = C::NPAD, KPAD = C::KPAD, AHALF = KPAD / 2;
+    constexpr int HEAD = C::HEAD, G0 = C::G0;
+    constexpr int BIMG = NPAD * KPAD * 2;            /* one fp16 B image */
+    /* shared memory: B hi/lo | barriers | tmem slot | harmonic headers; the
+     * rest of the SM's 256 KB stays L1 for the weight and spectrum reads */
+    constexpr int SM_B = 0, SM_BAR = 2 * BIMG, SM_TM = SM_BAR + 64, SM_HARM = SM_TM + 16;
+    static_assert(SM_HARM + NH * (int)sizeof(Harm) == smem_bytes<C>(), "layout");
+    static_assert(NH % 4 == 0 && 2 * NH <= KPAD && KPAD % 16 == 0 && NPAD <= D_STRIDE &&
+                  NPAD % 16 == 0 && HEAD + G0 <= NH / 4, "shape");
     extern __shared__ __align__(1024) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t bar_afull = smem_u32(smem + SM_BAR);        /* 2 x 8 B */
@@ -475,12 +619,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const __grid_constant
         const int par = tid >> 7;
         const uint32_t tlane = (uint32_t)((warp & 3) * 32) << 16;
         if (par == 1) {
-            /* the K padding block (k = 120..127) of both A buffers stays zero */
+            /* the K padding columns (harmonics past nharms) of both A buffers stay zero */
 #pragma unroll
             for (int b = 0; b < 2; b++) {
-                const uint32_t ab = tmem + tlane + (uint32_t)(TM_A + 128 * b);
-                tmem_st4(ab + 60, 0, 0, 0, 0);
-                tmem_st4(ab + 64 + 60, 0, 0, 0, 0);
+                const uint32_t ab = tmem + tlane + (uint32_t)(TM_A + KPAD * b);
+#pragma unroll
+                for (int c = NH; c < AHALF; c += 4) {
+                    tmem_st4(ab + c, 0, 0, 0, 0);
+                    tmem_st4(ab + AHALF + c, 0, 0, 0, 0);
+                }
             }
         }
         int it = 0;
@@ -492,12 +639,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const __grid_constant
             }
             tc_fence_after();
             const TrialState ts = trial_state(a, tile, r);
-            const uint32_t abuf = tmem + tlane + (uint32_t)(TM_A + 128 * s);
+            const uint32_t abuf = tmem + tlane + (uint32_t)(TM_A + KPAD * s);
             uint32_t res, qint, r4, q4;
             state_at(a, ts, 4u * par + 1u, res, qint);
             state_at(a, ts, 4u, r4, q4);     /* step of 4 harmonics */
             for (int hb = par; hb < HEAD; hb += 2) {
-                interp_block(a, hs, ts, hb, res, qint, scale, abuf);
+                interp_block<AHALF>(a, hs, ts, hb, res, qint, scale, abuf);
                 res += r4; qint += q4;       /* 4hb+5 -> 4(hb+2)+1 */
                 if (res >= (uint32_t)a.q) { res -= (uint32_t)a.q; qint += 1; }
             }
@@ -507,7 +654,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const __grid_constant
             if (lane == 0) mbar_arrive(bar_afull + 8 * s);
         }
     } else {
-        /* ----- tensor cores, epilogue, and blocks HEAD..14 of the next tile ---- */
+        /* ----- tensor cores, epilogue, and blocks HEAD.. of the next tile ---- */
         const int e = warp - 8;
         const int quarter = e & 3, grp = e >> 2;
         const int r = quarter * 32 + lane;
@@ -525,10 +672,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const __grid_constant
 
         auto tail = [&](int it, int tile) {
             const TrialState ts = trial_state(a, tile, r);
-            const uint32_t abuf = tmem + tlane + (uint32_t)(TM_A + 128 * (it & 1));
+            const uint32_t abuf = tmem + tlane + (uint32_t)(TM_A + KPAD * (it & 1));
             uint32_t res, qint;
             state_at(a, ts, 4u * tb0 + 1u, res, qint);
-            for (int hb = tb0; hb < tb1; hb++) interp_block(a, hs, ts, hb, res, qint, scale, abuf);
+            for (int hb = tb0; hb < tb1; hb++)
+                interp_block<AHALF>(a, hs, ts, hb, res, qint, scale, abuf);
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             tc_fence_before();
             __syncwarp();
@@ -538,8 +686,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const __grid_constant
             const int s = it & 1;
             if (!mbar_wait(bar_afull + 8 * s, (it >> 1) & 1)) return false;
             tc_fence_after();
-            const uint32_t a_hi = tmem + (uint32_t)(TM_A + 128 * s), a_lo = a_hi + 64;
-            const uint32_t d = tmem + (uint32_t)(TM_D + 128 * s);
+            const uint32_t a_hi = tmem + (uint32_t)(TM_A + KPAD * s), a_lo = a_hi + AHALF;
+            const uint32_t d = tmem + (uint32_t)(TM_D + D_STRIDE * s);
             uint32_t acc = 0;
 #pragma unroll
             for (int pass = 0; pass < 3; pass++) {
@@ -594,32 +742,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const __grid_constant
             const CsChunk &ch = a.chunks[ci];
             const bool valid = r < cnt;
             const int j = j0 + r;
-            const uint32_t trow = tmem + (uint32_t)(TM_D + s * 128) + ((uint32_t)(quarter * 32) << 16);
-            if (grp == 0) {
-                float iv[5], iw[4];
-#pragma unroll
-                for (int q = 0; q < 5; q++) iv[q] = ch.invsw[0][q];
-#pragma unroll
-                for (int q = 0; q < 4; q++) iw[q] = ch.invsw[5][q];
-                const float m0 = base_metric(trow, iv) * inv_scale;
-                const float m5 = fold_metric<6>(trow, iw) * inv_scale;
-                emit(a, valid && j < ch.nvalid[0] && (double)m0 > a.thresh, ci, 0, j, m0, lane);
-                emit(a, valid && j < ch.nvalid[5] && (double)m5 > a.thresh, ci, 5, j, m5, lane);
-            } else {
-                float iw[4][4];
-#pragma unroll
-                for (int sl = 0; sl < 4; sl++)
-#pragma unroll
-                    for (int q = 0; q < 4; q++) iw[sl][q] = ch.invsw[sl + 1][q];
-                const float m1 = fold_metric<2>(trow, iw[0]) * inv_scale;
-                emit(a, valid && j < ch.nvalid[1] && (double)m1 > a.thresh, ci, 1, j, m1, lane);
-                const float m2 = fold_metric<3>(trow, iw[1]) * inv_scale;
-                emit(a, valid && j < ch.nvalid[2] && (double)m2 > a.thresh, ci, 2, j, m2, lane);
-                const float m3 = fold_metric<4>(trow, iw[2]) * inv_scale;
-                emit(a, valid && j < ch.nvalid[3] && (double)m3 > a.thresh, ci, 3, j, m3, lane);
-                const float m4 = fold_metric<5>(trow, iw[3]) * inv_scale;
-                emit(a, valid && j < ch.nvalid[4] && (double)m4 > a.thresh, ci, 4, j, m4, lane);
-            }
+            const uint32_t trow = tmem + (uint32_t)(TM_D + s * D_STRIDE) + ((uint32_t)(quarter * 32) << 16);
+            C::epilogue(grp, trow, ch, a, valid, ci, j, lane, inv_scale);
             tc_fence_before();
             epi_bar_and(true);      /* accumulator s free for the MMA of tile it+2 */
         }
@@ -636,4 +760,4 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws60(const __grid_constant
     }
 }
 
-}  // namespace ws60
+}  // namespace wsk

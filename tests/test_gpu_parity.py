@@ -8,6 +8,9 @@ Tolerances (stated here, applied below):
   * a candidate may appear on one side only if its S/N lies within 1e-3
     (relative) of the threshold (a documented threshold flip).
 """
+import glob
+import os
+
 import numpy as np
 import pytest
 
@@ -43,8 +46,8 @@ def match_candidates(a, b, thr, rtol):
     return only_a, only_b
 
 
-@pytest.mark.parametrize("nharms,kernel", [(60, "ws"), (60, "generic"), (32, "generic"),
-                                           (16, "generic"), (7, "generic")])
+@pytest.mark.parametrize("nharms,kernel", [(60, "ws"), (32, "ws"), (16, "ws"), (60, "generic"),
+                                           (32, "generic"), (16, "generic"), (7, "generic")])
 def test_all_trial_metrics_vs_oracle(gpu_ready, monkeypatch, nharms, kernel):
     """Every trial of every decimation slot: GPU metric vs the oracle's."""
     if kernel == "generic":
@@ -80,6 +83,27 @@ def test_candidates_vs_reference_small(gpu_ready):
     raw_sorted = raw[np.argsort(raw["freq"], kind="stable")]
     match_candidates(raw_sorted, ref_sorted, 6.0, SNR_RTOL_F32)
     ses.close()
+
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_candidates_vs_golden(gpu_ready, path):
+    """Raw candidates against the reference's own, stored in the fixtures
+    (nharms 60 and 32 take the warp-specialised kernels, the hidr 0.25 case
+    the generic one)."""
+    z = np.load(path, allow_pickle=False)
+    o = {k[4:]: z[k].item() for k in z.files if k.startswith("opt_")}
+    opts = Options(**o)
+    ses = Session(int(z["N"]), float(z["dt"]), opts)
+    try:
+        raw = ses.run_raw(z["amps"])
+    finally:
+        ses.close()
+    raw = raw[np.argsort(raw["freq"], kind="stable")]
+    match_candidates(raw, z["raw"], opts.threshold, SNR_RTOL_F32)
+    match_candidates(raw, z["raw64"], opts.threshold, SNR_RTOL_F64)
 
 
 def test_config_small_end_to_end(gpu_ready):
