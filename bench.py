@@ -582,13 +582,16 @@ def run_sweep(args):
                 e1.synchronize()
                 ts.append(e0.elapsed_time(e1))
             res[name] = (statistics.mean(ts), out)
-        equal = all(_same_cands(x, y) for x, y in zip(res["plain"][1], res["batched"][1]))
+        diff = [i for i, (x, y) in enumerate(zip(res["plain"][1], res["batched"][1]))
+                if not _same_cands(x, y)]
+        equal = not diff
         lines[nh] = {"trials": trials, "plain_ms": res["plain"][0], "batched_ms": res["batched"][0],
                      "plain_trials_per_s": trials / (res["plain"][0] * 1e-3),
                      "batched_trials_per_s": trials / (res["batched"][0] * 1e-3),
                      "batched_vs_plain": res["plain"][0] / res["batched"][0],
-                     "equal_candidates": bool(equal),
-                     "candidates": int(sum(o.size for o in res["batched"][1]))}
+                     "equal_candidates": bool(equal), "differing_files": diff,
+                     "candidates": int(sum(o.size for o in res["batched"][1])),
+                     "plain_candidates": int(sum(o.size for o in res["plain"][1]))}
     h2d = int(sum(a.nbytes for a in spectra))
     main = lines[60]
     line = {

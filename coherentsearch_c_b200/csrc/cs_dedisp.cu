@@ -603,6 +603,9 @@ CS_EXPORT CsDedisp *cs_dedisp_create(int nchan, int nsub, int ndm, const int *id
                                   (int)dm_smem));
     DDCK(cudaFuncSetAttribute(dd::dd_subband_u8, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               max_optin));
+    /* a copy from pageable memory may return before its DMA lands; finish
+     * them all before a run on any stream can read the tables */
+    DDCK(cudaDeviceSynchronize());
 #undef DDCK
     return D;
 }

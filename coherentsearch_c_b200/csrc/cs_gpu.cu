@@ -892,33 +892,29 @@ static int session_load(GpuSession *S, const FFTFile *ft, const SearchParams *p,
     }
     const CsTables &t = S->tab;
     CK(dev_reserve((void **)&S->d_amps, &S->c_amps, (size_t)S->namps * sizeof(float2)));
-    CK(cudaMemcpy(S->d_harm, t.harm, sizeof(CsHarm) * CS_MAX_NH, cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(S->d_harm, t.harm, sizeof(CsHarm) * CS_MAX_NH, cudaMemcpyHostToDevice, S->st));
     CK(dev_reserve((void **)&S->d_rowtab, &S->c_rowtab, (size_t)t.nh * t.q * sizeof(uint16_t)));
-    CK(cudaMemcpy(S->d_rowtab, t.rowtab, (size_t)t.nh * t.q * sizeof(uint16_t),
-                  cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(S->d_rowtab, t.rowtab, (size_t)t.nh * t.q * sizeof(uint16_t), cudaMemcpyHostToDevice, S->st));
     CK(dev_reserve((void **)&S->d_W, &S->c_W, (size_t)t.nrows * t.m * sizeof(float)));
-    CK(cudaMemcpy(S->d_W, t.W, (size_t)t.nrows * t.m * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(S->d_W, t.W, (size_t)t.nrows * t.m * sizeof(float), cudaMemcpyHostToDevice, S->st));
     CK(dev_reserve((void **)&S->d_A, &S->c_A, (size_t)t.nrows * sizeof(float2)));
-    CK(cudaMemcpy(S->d_A, t.A, (size_t)t.nrows * sizeof(float2), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(S->d_A, t.A, (size_t)t.nrows * sizeof(float2), cudaMemcpyHostToDevice, S->st));
     CK(dev_reserve((void **)&S->d_carry, &S->c_carry, (size_t)t.nrows));
-    CK(cudaMemcpy(S->d_carry, t.carry, (size_t)t.nrows, cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(S->d_carry, t.carry, (size_t)t.nrows, cudaMemcpyHostToDevice, S->st));
     CK(dev_reserve((void **)&S->d_chunks, &S->c_chunks, (size_t)nchunks * sizeof(CsChunk)));
     if (nchunks > 0)
-        CK(cudaMemcpy(S->d_chunks, t.chunks, (size_t)nchunks * sizeof(CsChunk),
-                      cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(S->d_chunks, t.chunks, (size_t)nchunks * sizeof(CsChunk), cudaMemcpyHostToDevice, S->st));
     CK(dev_reserve((void **)&S->d_tiles, &S->c_tiles, (size_t)t.ntiles * 3 * sizeof(int)));
     if (t.ntiles > 0)
-        CK(cudaMemcpy(S->d_tiles, t.tiles, (size_t)t.ntiles * 3 * sizeof(int),
-                      cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(S->d_tiles, t.tiles, (size_t)t.ntiles * 3 * sizeof(int), cudaMemcpyHostToDevice, S->st));
     img_halves = (size_t)t.npad * t.kpad;
     bhi.resize(img_halves);
     blo.resize(img_halves);
     cs_tables_dft_images(&S->tab, bhi.data(), blo.data());
     S->bbytes = (int)(img_halves * 2);
     CK(dev_reserve((void **)&S->d_bimg, &S->c_bimg, (size_t)2 * S->bbytes));
-    CK(cudaMemcpy(S->d_bimg, bhi.data(), (size_t)S->bbytes, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy((char *)S->d_bimg + S->bbytes, blo.data(), (size_t)S->bbytes,
-                  cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(S->d_bimg, bhi.data(), (size_t)S->bbytes, cudaMemcpyHostToDevice, S->st));
+    CK(cudaMemcpyAsync((char *)S->d_bimg + S->bbytes, blo.data(), (size_t)S->bbytes, cudaMemcpyHostToDevice, S->st));
     S->use_ws = ws_config(t, total);
     if (S->use_ws && (S->namps >= 2147483000LL || ws_smem(S->use_ws) > S->max_smem))
         S->use_ws = 0;
@@ -941,9 +937,9 @@ static int session_load(GpuSession *S, const FFTFile *ft, const SearchParams *p,
                         t.W[(size_t)(off + ph) * t.m + i];
         }
         if (!S->d_harm2) CK(cudaMalloc((void **)&S->d_harm2, sizeof(wsk::Harm) * wsk::MAX_NH));
-        CK(cudaMemcpy(S->d_harm2, S->hh, sizeof(wsk::Harm) * t.nh, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(S->d_harm2, S->hh, sizeof(wsk::Harm) * t.nh, cudaMemcpyHostToDevice, S->st));
         if (!S->d_Wt) CK(cudaMalloc((void **)&S->d_Wt, nq * sizeof(float4)));
-        CK(cudaMemcpy(S->d_Wt, wfix.data(), wfix.size() * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(S->d_Wt, wfix.data(), wfix.size() * sizeof(float), cudaMemcpyHostToDevice, S->st));
         CK(ws_prepare(S->use_ws));
     }
     {
@@ -958,6 +954,12 @@ static int session_load(GpuSession *S, const FFTFile *ft, const SearchParams *p,
      * never lowered to this geometry's need */
     CK(set_smem_cap((const void *)cs_search_kernel<16>, S->max_smem));
     CK(set_smem_cap((const void *)cs_search_kernel<0>, S->max_smem));
+    /* The uploads are ordered on the session stream and finished here: a
+     * synchronous copy from pageable memory may return before its DMA lands,
+     * and nothing would order that DMA before a kernel on a non-blocking
+     * stream -- with reused buffers the kernel could read the previous
+     * geometry's tables.  The host tables and vectors may go after this. */
+    CK(cudaStreamSynchronize(S->st));
     return 0;
 fail:
     return -1;
