@@ -820,11 +820,11 @@ static cudaError_t ws_prepare(int nh)
 static void ws_launch(int nh, int grid, cudaStream_t st, const wsk::Args &w)
 {
     if (nh == 60)
-        wsk::search_ws<wsk::Cfg60><<<grid, wsk::NTHREADS, ws_smem(60), st>>>(w);
+        wsk::search_ws<wsk::Cfg60><<<grid, wsk::nthreads<wsk::Cfg60>(), ws_smem(60), st>>>(w);
     else if (nh == 32)
-        wsk::search_ws<wsk::Cfg32><<<grid, wsk::NTHREADS, ws_smem(32), st>>>(w);
+        wsk::search_ws<wsk::Cfg32><<<grid, wsk::nthreads<wsk::Cfg32>(), ws_smem(32), st>>>(w);
     else
-        wsk::search_ws<wsk::Cfg16><<<grid, wsk::NTHREADS, ws_smem(16), st>>>(w);
+        wsk::search_ws<wsk::Cfg16><<<grid, wsk::nthreads<wsk::Cfg16>(), ws_smem(16), st>>>(w);
 }
 
 static uint32_t magic_for(int d)

@@ -4,16 +4,16 @@
  * configuration per harmonic count (the profile columns, the width banks of
  * each decimation and how the epilogue splits them; see Cfg60/Cfg32/Cfg16).
  *
- * One persistent CTA per SM, 16 warps:
- *   warps 0-7   interpolation of harmonic blocks 0..HEAD-1 of tile i into
+ * One persistent CTA per SM; NIW (8 or 16) interpolation warps, then 8:
+ *   warps 0..NIW-1  interpolation of harmonic blocks 0..HEAD-1 of tile i into
  *               the fp16 hi/lo A operand in tensor-memory buffer i%2 (same
  *               FP32 arithmetic as the generic kernel, bit-identical
  *               harmonic amplitudes);
- *   warps 8-15  the remaining harmonic blocks of tile i+1, tensor-core issue
+ *   the last 8  the remaining harmonic blocks of tile i+1, tensor-core issue
  *               (one elected thread), then the boxcar epilogue of tile i from
  *               tensor-memory accumulator i%2.  The split evens out the two
  *               roles' instruction counts per tile.
- * Hand-off through mbarriers: a_full (16 warp arrivals), a_empty and d_full
+ * Hand-off through mbarriers: a_full (one arrival per warp), a_empty and d_full
  * (tcgen05.commit).  The epilogue keeps every prefix sum in registers: with
  * the bin count and widths known at compile time, the cyclic prefix, the
  * sliding window differences P[i] - P[i-w] and the k-fold sums all unroll
@@ -27,7 +27,17 @@
 namespace wsk {
 
 constexpr int M = 16;               /* interpolation taps */
-constexpr int NTHREADS = 512;
+/* interpolation warps per CTA (8 or 16; WSK_NIW* override them for tuning
+ * builds); the epilogue always has 8 */
+#ifndef WSK_NIW60
+#define WSK_NIW60 8
+#endif
+#ifndef WSK_NIW32
+#define WSK_NIW32 8
+#endif
+#ifndef WSK_NIW16
+#define WSK_NIW16 8
+#endif
 constexpr int MAX_NH = 60;
 /* tensor memory (512 columns): accumulators D0, D1 at columns 0 and 128
  * (N <= 128); operands A0, A1 (hi: K/2 columns, then lo: K/2 columns) from
@@ -483,7 +493,7 @@ using W2 = Widths<2, 3>;
  * with the width banks (src/boxcar.c:100-133) written out below.  Each
  * group's epilogue work is balanced against its share of the blocks. */
 struct Cfg60 {
-    static constexpr int NH = 60, NPAD = 128, KPAD = 128, HEAD = 12, G0 = 2;
+    static constexpr int NH = 60, NPAD = 128, KPAD = 128, HEAD = 12, G0 = 2, NIW = WSK_NIW60;
     static __device__ __forceinline__ void epilogue(int grp, uint32_t trow, const CsChunk &ch,
                                                     const Args &a, bool valid, int ci, int j,
                                                     int lane, float inv)
@@ -501,7 +511,7 @@ struct Cfg60 {
 };
 
 struct Cfg32 {
-    static constexpr int NH = 32, NPAD = 112, KPAD = 64, HEAD = 6, G0 = 1;
+    static constexpr int NH = 32, NPAD = 112, KPAD = 64, HEAD = 6, G0 = 1, NIW = WSK_NIW32;
     static __device__ __forceinline__ void epilogue(int grp, uint32_t trow, const CsChunk &ch,
                                                     const Args &a, bool valid, int ci, int j,
                                                     int lane, float inv)
@@ -519,7 +529,7 @@ struct Cfg32 {
 };
 
 struct Cfg16 {
-    static constexpr int NH = 16, NPAD = 64, KPAD = 32, HEAD = 3, G0 = 1;
+    static constexpr int NH = 16, NPAD = 64, KPAD = 32, HEAD = 3, G0 = 1, NIW = WSK_NIW16;
     static __device__ __forceinline__ void epilogue(int grp, uint32_t trow, const CsChunk &ch,
                                                     const Args &a, bool valid, int ci, int j,
                                                     int lane, float inv)
@@ -561,15 +571,23 @@ static const CfgDesc kCfgDescs[3] = {
 };
 
 template <class C>
+__host__ __device__ constexpr int nthreads()
+{
+    return (C::NIW + 8) * 32;
+}
+
+template <class C>
 __host__ __device__ constexpr int smem_bytes()
 {
     return 2 * C::NPAD * C::KPAD * 2 + 64 + 16 + C::NH * (int)sizeof(Harm);
 }
 
 template <class C>
-__global__ void __launch_bounds__(NTHREADS, 1) search_ws(const __grid_constant__ Args a)
+__global__ void __launch_bounds__(nthreads<C>(), 1) search_ws(const __grid_constant__ Args a)
 {
     constexpr int NH = C::NH, NPAD = C::NPAD, KPAD = C::KPAD, AHALF = KPAD / 2;
+    constexpr int NIW = C::NIW, NPAR = NIW / 4, NTHREADS = nthreads<C>();
+    static_assert(NIW == 8 || NIW == 16, "interpolation warps");
     constexpr int HEAD = C::HEAD, G0 = C::G0;
     constexpr int BIMG = NPAD * KPAD * 2;            /* one fp16 B image */
     /* shared memory: B hi/lo | barriers | tmem slot | harmonic headers; the
@@ -589,8 +607,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws(const __grid_constant__
     if (warp == 0) tmem_alloc(smem_u32(tm_slot), TMEM_COLS);
     for (int h = tid; h < NH; h += NTHREADS) hs[h] = a.harm[h];
     if (tid == 0) {
-        mbar_init(bar_afull, 16);      /* 8 interpolation + 8 epilogue warps */
-        mbar_init(bar_afull + 8, 16);
+        mbar_init(bar_afull, NIW + 8);      /* every interpolation and epilogue warp */
+        mbar_init(bar_afull + 8, NIW + 8);
         mbar_init(bar_aempty, 1);
         mbar_init(bar_aempty + 8, 1);
         mbar_init(bar_dfull, 1);
@@ -613,7 +631,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws(const __grid_constant__
     const int tile_begin = min(a.ntiles, (int)blockIdx.x * per_cta);
     const int tile_end = min(a.ntiles, tile_begin + per_cta);
 
-    if (warp < 8) {
+    if (warp < NIW) {
         /* --------------- interpolation of blocks 0..HEAD-1 --------------- */
         const int r = tid & (CS_TILE_M - 1);
         const int par = tid >> 7;
@@ -642,10 +660,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws(const __grid_constant__
             const uint32_t abuf = tmem + tlane + (uint32_t)(TM_A + KPAD * s);
             uint32_t res, qint, r4, q4;
             state_at(a, ts, 4u * par + 1u, res, qint);
-            state_at(a, ts, 4u, r4, q4);     /* step of 4 harmonics */
-            for (int hb = par; hb < HEAD; hb += 2) {
+            state_at(a, ts, 4u * (NPAR - 1), r4, q4);   /* the harmonics other groups take */
+            for (int hb = par; hb < HEAD; hb += NPAR) {
                 interp_block<AHALF>(a, hs, ts, hb, res, qint, scale, abuf);
-                res += r4; qint += q4;       /* 4hb+5 -> 4(hb+2)+1 */
+                res += r4; qint += q4;       /* 4hb+5 -> 4(hb+NPAR)+1 */
                 if (res >= (uint32_t)a.q) { res -= (uint32_t)a.q; qint += 1; }
             }
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
@@ -655,11 +673,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) search_ws(const __grid_constant__
         }
     } else {
         /* ----- tensor cores, epilogue, and blocks HEAD.. of the next tile ---- */
-        const int e = warp - 8;
+        const int e = warp - NIW;
         const int quarter = e & 3, grp = e >> 2;
         const int r = quarter * 32 + lane;
         const uint32_t tlane = (uint32_t)(quarter * 32) << 16;
-        const bool leader = (warp == 8 && lane == 0);
+        const bool leader = (warp == NIW && lane == 0);
         const uint32_t idesc = (1u << 4) | ((uint32_t)(NPAD >> 3) << 17) |
                                ((uint32_t)(CS_TILE_M >> 4) << 24);
         const uint32_t lbo_b = NPAD * 16;
