@@ -33,7 +33,7 @@ CFLAGS = ["-O2", "-fPIC", "-std=gnu11", "-ffp-contract=off", "-Wall", "-Wextra",
 HOST_COMMON = ["cs_common.c"]
 HOST_GPU_ONLY = ["cs_tables.c"]
 HOST_LIB = ["cs_common.c", "cs_search.c"]
-CUDA_SRCS = ["cs_gpu.cu", "cs_dedisp.cu"]
+CUDA_SRCS = ["cs_gpu.cu", "cs_dedisp.cu", "cs_spectrum.cu"]
 
 
 def _run(cmd, verbose):
@@ -85,7 +85,9 @@ def build(verbose: bool = False, force: bool = False) -> None:
         gpu_objs.append(o)
     libgpu = os.path.join(LIB, "libcsgpu.so")
     if force or _newer(libgpu, gpu_objs):
-        _run([NVCC] + GENCODE + ["-shared", "-o", libgpu] + gpu_objs, verbose)
+        cudalib = os.path.join(os.path.dirname(os.path.dirname(NVCC)), "lib64")
+        _run([NVCC] + GENCODE + ["-shared", "-o", libgpu] + gpu_objs +
+             [f"-L{cudalib}", "-lcufft", "-Xlinker", f"-rpath={cudalib}"], verbose)
 
     # host library (exports the coherent_search.h host API)
     host_objs = []

@@ -162,6 +162,14 @@ def declare_gpu_api(lib: C.CDLL) -> C.CDLL:
     lib.cs_gpu_batch_pending.argtypes = [C.c_void_p]
     lib.cs_gpu_batch_pending.restype = C.c_int
     lib.cs_gpu_batch_free.argtypes = [C.c_void_p]
+    lib.cs_spectrum_create.argtypes = [C.c_longlong, C.c_double, C.c_int, C.c_int, C.c_double,
+                                       C.c_int]
+    lib.cs_spectrum_create.restype = C.c_void_p
+    lib.cs_spectrum_run_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.cs_spectrum_run_device.restype = C.c_int
+    lib.cs_spectrum_run.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.cs_spectrum_run.restype = C.c_int
+    lib.cs_spectrum_free.argtypes = [C.c_void_p]
     IP = P(C.c_int)
     lib.cs_dedisp_tables.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                      C.c_double, C.c_double, C.c_double, C.c_int, IP, IP, IP,

@@ -87,6 +87,27 @@ int cs_gpu_batch_pending(CsBatch *b);
  * for are dropped). */
 void cs_gpu_batch_free(CsBatch *b);
 
+/* ---- time series -> normalised spectrum ---------------------------------
+ * The in-memory `realfft + rednoise` of src/datpipe.c:101-253: forward real
+ * FFT packed PRESTO-style (bin 0 = DC, Nyquist), then the running block-median
+ * normalisation (defaults startwidth 6, endwidth 100, endfreq 6 Hz,
+ * src/cli.c).  Output: N/2 complex bins (interleaved floats), the layout of
+ * FFTFile.amps and of a session's device spectrum.  One run at a time per
+ * plan.  NULL / -1 where the reference's rednoise stops with an error. */
+typedef struct CsSpectrum CsSpectrum;
+
+CsSpectrum *cs_spectrum_create(long long N, double dt, int startwidth, int endwidth,
+                               double endfreq, int device);
+
+/* Device buffers: d_series N floats, d_amps N floats (N/2 complex); on
+ * `stream` (a cudaStream_t; NULL: the plan's stream). */
+int cs_spectrum_run_device(CsSpectrum *s, const float *d_series, float *d_amps, void *stream);
+
+/* Host buffers; copies in and out and waits. */
+int cs_spectrum_run(CsSpectrum *s, const float *h_series, float *h_amps);
+
+void cs_spectrum_free(CsSpectrum *s);
+
 /* ---- subband dedispersion of 8-bit filterbank data ---------------------
  * The prepsubband stage of the reference's raw-data front end
  * (src/prep_dedisp.c:444-466 tables, :1104-1275 block driver; PRESTO

@@ -29,10 +29,11 @@ def test_gpu_library_exports_match_headers():
     lib = os.path.join(nt.LIBDIR, "libcsgpu.so")
     exp = exported(lib)
     want = declared("coherent_search.h", "cs_gpu_") | declared("cs_b200.h", "cs_b200_")
-    want |= declared("cs_b200.h", "cs_dedisp_")
+    want |= declared("cs_b200.h", "cs_dedisp_") | declared("cs_b200.h", "cs_spectrum_")
     assert want <= exp, sorted(want - exp)
     # nothing else leaks: the host helpers inside libcsgpu.so are hidden
-    extra = {s for s in exp if not s.startswith(("cs_gpu_", "cs_b200_", "cs_dedisp_"))}
+    extra = {s for s in exp
+             if not s.startswith(("cs_gpu_", "cs_b200_", "cs_dedisp_", "cs_spectrum_"))}
     assert not extra, sorted(extra)
 
 
