@@ -140,7 +140,8 @@ def cpu_reference_rate(amps, N, seconds=10.0, max_reps=50):
     opts = Options(blocksize=2048, threshold=8.0)
     _, _, total = opts.geometry(N, WORKLOAD["dt"])
     cores = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    rb.ref_lib()
+    rb.pin_ref_threads(cores)                          # speed, not parity: every host thread
     rb.ref_search(amps, N, WORKLOAD["dt"], opts)      # warm (plans, pages)
     t0 = time.perf_counter()
     reps = 0
@@ -496,6 +497,159 @@ def run_dedisp(args):
     return 0
 
 
+def prep_cpu_rate(series_host, dd_rate, N, dt, opts, seconds=10.0):
+    """The reference CPU path of one DM on the host cores: its dedispersion
+    cost per DM at the measured dispersion.c rate (one thread, as
+    prepsubband runs it), plus realfft + rednoise and the OpenMP search of
+    full-length dedispersed series, repeated for about `seconds`.  Returns
+    (trials/s, cores, sample)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import refbind as rb
+    cores = os.cpu_count() or 1
+    rb.ref_lib()
+    rb.pin_ref_threads(cores)
+    _, _, total = opts.geometry(N, dt)
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        x = series_host[reps % len(series_host)]
+        amps = rb.ref_spectrum(x, dt)
+        rb.ref_search(amps, N, dt, opts)
+        reps += 1
+        if time.perf_counter() - t0 >= seconds or reps >= 8:
+            break
+    per_dm = (time.perf_counter() - t0) / reps + N / dd_rate
+    return total / per_dm, cores, (f"{reps} DM series of {N} points: realfft + rednoise + search "
+                                   f"(OpenMP, {cores} threads), plus {N} dedispersed samples "
+                                   f"per DM at the reference dispersion rate {dd_rate:.3g}/s")
+
+
+def run_prep(args):
+    """Raw-data front end end to end on one GPU: 8-bit filterbank ->
+    subband dedispersion (500 DMs) -> padding -> realfft + rednoise ->
+    coherent search of every DM (nharms 60, m 16)."""
+    import torch
+    from coherentsearch_c_b200 import synth
+    from coherentsearch_c_b200.dedisp import dedisp_tables
+    from coherentsearch_c_b200.prep import PrepSearch
+    from coherentsearch_c_b200.search import Options
+    world, rank, local, pg = dist_setup(args)
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    W = dict(DEDISP)
+    if args.nspec_log2:
+        W["nspec"] = W["numout"] = 1 << args.nspec_log2
+        W["workload"] = W["workload"].replace("2^22 spectra", f"2^{args.nspec_log2} spectra")
+    if args.ndm:
+        W["ndm"] = args.ndm
+        W["workload"] = W["workload"].replace("500 DMs 0-199.6", f"{args.ndm} DMs from 0")
+    spec = synth.config_filterbank(nspec=W["nspec"], seed=4 + rank)
+    t = dedisp_tables(W["nchan"], W["nsub"], W["ndm"], W["lodm"], W["dmstep"], spec.lofreq,
+                      spec.chanwid, spec.dt)
+    opts = Options(nharms=60, m=16, blocksize=65536, threshold=8.0)
+    raw = make_filterbank_device(spec, dev)
+    ps = PrepSearch(t, spec.nspec, W["numout"], spec.dt, opts, device=local)
+    N, total = ps.N, ps.ses.total
+    stream = ps.stream
+
+    def step():
+        ps.dedisperse(raw.data_ptr(), spec.nspec)
+        return ps.search_all()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+    times, dd_ms, search_ms, ncand = [], [], [], 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            res = step()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            a, b = ps.dd.last_times()
+            dd_ms.append(a + b)
+            search_ms.append(sum(ps.search_ms))
+            ncand = sum(r.size for r in res)
+        torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+    ms = statistics.mean(times)
+    if pg is not None:
+        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        ms = float(tt.item())
+    trials = t.ndm * total
+    value = world * trials / (ms * 1e-3)
+    hbm_peak, tc_peak, peak_kind = load_peaks()
+    kms = statistics.mean(search_ms)
+    dft_tflops = trials * DFT_FLOP_PER_TRIAL / (kms * 1e-3) / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8->f32",
+        "data": "synthetic",
+        "config": dict(workload=W["workload"] + "; search of every DM: N=" + str(N)
+                       + " (numout), nharms 60, m 16, hidr 0.5, 0.1-125 Hz, maxdecim 6, "
+                       "blocksize 65536, threshold 8", ndm=t.ndm, trials_per_dm=total,
+                       output_per_dm=ps.nout,
+                       l2="inputs larger than L2 (raw input and dedispersed output > 126 MB)",
+                       parallelism=f"replicas{world}"),
+        "gpu_launches": (2 + 6 * t.ndm) * args.steps,
+        "roofline": {"bound": "tensor", "achieved": dft_tflops, "peak": tc_peak,
+                     "unit": "TFLOP/s", "frac": dft_tflops / tc_peak, "traffic": None,
+                     "kernel": "search_ws60", "kernel_ms_per_dm": kms / t.ndm,
+                     "peak_kind": f"bf16 dense, {peak_kind}",
+                     "algorithmic": f"{DFT_FLOP_PER_TRIAL:.0f} DFT flop/trial x {total} trials "
+                                    f"x {t.ndm} DMs"},
+        "stages_ms": {"dedisp": statistics.mean(dd_ms), "search_kernels": kms,
+                      "rest": ms - statistics.mean(dd_ms) - kms},
+        "clocks": clk.summary(),
+        "candidates": ncand,
+    }
+    # end to end: pinned host filterbank in, every DM's candidates back
+    if not args.no_e2e:
+        h_raw = torch.empty(raw.shape, dtype=torch.uint8, pin_memory=True)
+        h_raw.copy_(raw)
+        e2e, nbytes_back = [], 0
+        for _ in range(max(2, args.steps // 2)):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            with torch.cuda.stream(stream):
+                raw.copy_(h_raw, non_blocking=True)
+            res = step()
+            e1.record(stream)
+            e1.synchronize()
+            e2e.append(e0.elapsed_time(e1))
+            nbytes_back = sum(r.nbytes for r in res)
+        line["e2e"] = {"value": world * trials / (statistics.mean(e2e) * 1e-3), "unit": UNIT,
+                       "h2d_bytes_per_step": int(h_raw.numel()),
+                       "d2h_bytes_per_step": int(nbytes_back)}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            nblk = 4 * t.blocks_per_read + 2
+            host = raw[: nblk * t.spectra_per_subint].cpu().numpy()
+            dd_rate, _, _ = dedisp_cpu_rate(host, t, seconds=max(2.0, args.cpu_seconds / 3))
+            ser = [ps.series(d) for d in (0, t.ndm // 2)]
+            rate, cores, sample = prep_cpu_rate(ser, dd_rate, N, spec.dt, opts,
+                                                seconds=args.cpu_seconds)
+            line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores,
+                                    "kind": "reference", "sample": sample}
+        except Exception as exc:   # noqa: BLE001
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0,
+                                    "kind": "reference", "sample": f"unavailable: {exc}"}
+    if rank == 0:
+        print(json.dumps(line))
+    ps.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
 def spectrum_device(N, dt, seed, pulsars, device):
     """A normalised spectrum as synth.normalised_spectrum builds it (white
     noise + von Mises pulse trains, PRESTO-packed forward FFT, unit power by
@@ -708,11 +862,12 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="search",
-                    choices=["search", "dedisp", "sweep", "serve"],
+                    choices=["search", "dedisp", "sweep", "serve", "prep"],
                     help="search: the coherent search (headline); dedisp: subband "
                          "dedispersion of the 8-bit filterbank workload; sweep: batched "
                          "search of a list of uneven-length files; serve: a Poisson "
-                         "stream of requests through the request loop")
+                         "stream of requests through the request loop; prep: the raw-data "
+                         "front end, filterbank -> dedispersion -> search of every DM")
     ap.add_argument("--files", type=int, default=256, help="sweep: number of files")
     ap.add_argument("--slots", type=int, default=3, help="sweep/serve: batch slots")
     ap.add_argument("--requests", type=int, default=800, help="serve: requests")
@@ -723,6 +878,8 @@ def main():
     ap.add_argument("--nspec-log2", type=int, default=0,
                     help="dedisp workload length 2^n spectra (default: the 2^22 workload; "
                          "smaller sizes are for profiling captures only)")
+    ap.add_argument("--ndm", type=int, default=0,
+                    help="prep: DM trials (default: the 500-DM workload; fewer for profiling)")
     ap.add_argument("--nlog2", type=int, default=23,
                     help="series length 2^n (23 = the benchmark workload; smaller "
                          "sizes are for profiling captures only)")
@@ -745,6 +902,13 @@ def main():
                               "object of its own line"}))
             return 0
         return run_dedisp(args)
+    if args.workload == "prep":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the front-end workload's reference arm is the cpu_baseline "
+                              "object of its own line"}))
+            return 0
+        return run_prep(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)

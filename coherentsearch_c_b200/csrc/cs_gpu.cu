@@ -631,6 +631,7 @@ struct GpuSession {
     int nsm;
     cudaStream_t st;
     cudaEvent_t ev0, ev1;
+    cudaEvent_t ev_in;        /* producer hand-off (enqueue_device's stream) */
     /* device buffers */
     float2 *d_amps;
     CsHarm *d_harm;
@@ -648,6 +649,8 @@ struct GpuSession {
     CsRec *d_recs;
     unsigned cap;
     unsigned *h_count;     /* pinned */
+    CsRec *h_recs;         /* pinned record staging, grown on demand */
+    size_t h_recs_cap;
     float last_kernel_ms;
     int own_plans;
     /* warp-specialised kernel (default ladder at nharms = 60) */
@@ -725,8 +728,10 @@ static void session_release(GpuSession *S)
     cudaFree(S->d_AC);
     cudaFree(S->d_harm2);
     if (S->h_count) cudaFreeHost(S->h_count);
+    if (S->h_recs) cudaFreeHost(S->h_recs);
     if (S->ev0) cudaEventDestroy(S->ev0);
     if (S->ev1) cudaEventDestroy(S->ev1);
+    if (S->ev_in) cudaEventDestroy(S->ev_in);
     if (S->st) cudaStreamDestroy(S->st);
     cs_tables_free(&S->tab);
     free(S);
@@ -990,6 +995,7 @@ static GpuSession *session_new(int device)
     CK(cudaStreamCreateWithFlags(&S->st, cudaStreamNonBlocking));
     CK(cudaEventCreate(&S->ev0));
     CK(cudaEventCreate(&S->ev1));
+    CK(cudaEventCreateWithFlags(&S->ev_in, cudaEventDisableTiming));
     CK(cudaMalloc((void **)&S->d_harm, sizeof(CsHarm) * CS_MAX_NH));
     CK(cudaMalloc((void **)&S->d_amax, 2 * sizeof(unsigned)));
     CK(cudaMalloc((void **)&S->d_count, sizeof(unsigned)));
@@ -1140,14 +1146,26 @@ static int collect(GpuSession *S, double threshold, CandidateList *out, int *nee
         return 0;
     }
     if (n == 0) return 0;
-    std::vector<CsRec> recs(n);
-    if ((e = cudaMemcpy(recs.data(), S->d_recs, (size_t)n * sizeof(CsRec),
-                        cudaMemcpyDeviceToHost)) != cudaSuccess) {
+    if ((size_t)n > S->h_recs_cap) {
+        const size_t cap = (size_t)n + n / 4 + 1024;
+        if (S->h_recs) cudaFreeHost(S->h_recs);
+        S->h_recs = NULL;
+        S->h_recs_cap = 0;
+        if ((e = cudaMallocHost((void **)&S->h_recs, cap * sizeof(CsRec))) != cudaSuccess) {
+            S->h_recs = NULL;
+            fprintf(stderr, "Error: B200 record staging: %s\n", cudaGetErrorString(e));
+            return -1;
+        }
+        S->h_recs_cap = cap;
+    }
+    if ((e = cudaMemcpyAsync(S->h_recs, S->d_recs, (size_t)n * sizeof(CsRec),
+                             cudaMemcpyDeviceToHost, S->st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(S->st)) != cudaSuccess) {
         fprintf(stderr, "Error: B200 search readback failed: %s\n", cudaGetErrorString(e));
         return -1;
     }
-    cs_sort_records(recs.data(), (long long)n);
-    cs_harvest(&S->tab, recs.data(), (long long)n, S->r_lo, S->lodr, (double)S->N, S->T,
+    cs_sort_records(S->h_recs, (long long)n);
+    cs_harvest(&S->tab, S->h_recs, (long long)n, S->r_lo, S->lodr, (double)S->N, S->T,
                threshold, out);
     return 0;
 }
@@ -1237,7 +1255,12 @@ CS_EXPORT int cs_b200_session_enqueue_device(GpuSession *S, const float *d_amps,
                                              double threshold, void *stream)
 {
     if (!S) return -1;
-    (void)stream;
+    if (stream) {
+        /* the spectrum is produced on the caller's stream: start after it */
+        if (cudaEventRecord(S->ev_in, (cudaStream_t)stream) != cudaSuccess ||
+            cudaStreamWaitEvent(S->st, S->ev_in, 0) != cudaSuccess)
+            return -1;
+    }
     cudaError_t e = enqueue_search(S, d_amps ? (const float2 *)d_amps : S->d_amps, threshold,
                                    true);
     return e == cudaSuccess ? 0 : -1;

@@ -637,3 +637,23 @@ CandidateList search_file(const FFTFile *ft, const SearchParams *p,
     }
     return cands;
 }
+
+/* ------------------------------------------------------------------ */
+/* prepsubband padding value                                          */
+/* ------------------------------------------------------------------ */
+/* The running mean of PRESTO's update_stats
+ * (third_party/presto/include/misc_utils.h:114-127) over n samples: each
+ * sample as a float, the mean in double, one step at a time.  prepsubband
+ * pads every DM series with it, taken over DM 0's samples
+ * (src/prep_dedisp.c:505-511, 774-790). */
+double cs_prep_pad_value(const float *x, long long n)
+{
+    double avg = 0.0;
+    long long i;
+    for (i = 0; i < n; i++) {
+        const float xbk = x[i];
+        const double dev = xbk - avg;
+        avg += dev / ((double)(int)i + 1.0);
+    }
+    return avg;
+}

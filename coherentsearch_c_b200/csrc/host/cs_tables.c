@@ -378,9 +378,71 @@ static int rec_cmp(const void *a, const void *b)
     return (x->j > y->j) - (x->j < y->j);
 }
 
+static int bit_length(unsigned v)
+{
+    int b = 0;
+    while (v) { b++; v >>= 1; }
+    return b;
+}
+
+/* Records into (chunk, slot, j) order.  Each (chunk, slot, j) is written at
+ * most once, so the order is total and any correct sort gives the same
+ * sequence; this one is an LSD radix sort on the packed key (11-bit digits,
+ * usually three passes), linear in n where a comparison sort of the tens of
+ * thousands of records a strong source gives would dominate the search. */
 CS_HIDDEN_API void cs_sort_records(CsRec *recs, long long n)
 {
-    if (n > 1) qsort(recs, (size_t)n, sizeof(CsRec), rec_cmp);
+    if (n < 2) return;
+    unsigned mc = 0, ms = 0, mj = 0;
+    long long i;
+    for (i = 0; i < n; i++) {
+        if (recs[i].chunk < 0 || recs[i].slot < 0 || recs[i].j < 0) {
+            qsort(recs, (size_t)n, sizeof(CsRec), rec_cmp);
+            return;
+        }
+        if ((unsigned)recs[i].chunk > mc) mc = (unsigned)recs[i].chunk;
+        if ((unsigned)recs[i].slot > ms) ms = (unsigned)recs[i].slot;
+        if ((unsigned)recs[i].j > mj) mj = (unsigned)recs[i].j;
+    }
+    const int bj = bit_length(mj), bs = bit_length(ms), bc = bit_length(mc);
+    const int bits = bj + bs + bc;
+    if (n < 256 || bits > 63) {
+        qsort(recs, (size_t)n, sizeof(CsRec), rec_cmp);
+        return;
+    }
+    uint64_t *key = (uint64_t *)malloc((size_t)n * 2 * sizeof(uint64_t));
+    CsRec *tmp = (CsRec *)malloc((size_t)n * sizeof(CsRec));
+    if (!key || !tmp) {
+        free(key); free(tmp);
+        qsort(recs, (size_t)n, sizeof(CsRec), rec_cmp);
+        return;
+    }
+    uint64_t *key2 = key + n;
+    for (i = 0; i < n; i++)
+        key[i] = ((uint64_t)(unsigned)recs[i].chunk << (bj + bs)) |
+                 ((uint64_t)(unsigned)recs[i].slot << bj) | (uint64_t)(unsigned)recs[i].j;
+    enum { DIG = 11, NB = 1 << DIG };
+    long long cnt[NB];
+    CsRec *src = recs, *dst = tmp;
+    uint64_t *ks = key, *kd = key2;
+    int shift;
+    for (shift = 0; shift < bits; shift += DIG) {
+        memset(cnt, 0, sizeof(cnt));
+        for (i = 0; i < n; i++) cnt[(ks[i] >> shift) & (NB - 1)]++;
+        long long sum = 0;
+        int d;
+        for (d = 0; d < NB; d++) { const long long c = cnt[d]; cnt[d] = sum; sum += c; }
+        for (i = 0; i < n; i++) {
+            const long long o = cnt[(ks[i] >> shift) & (NB - 1)]++;
+            dst[o] = src[i];
+            kd[o] = ks[i];
+        }
+        CsRec *tr = src; src = dst; dst = tr;
+        uint64_t *tk = ks; ks = kd; kd = tk;
+    }
+    if (src != recs) memcpy(recs, src, (size_t)n * sizeof(CsRec));
+    free(key);
+    free(tmp);
 }
 
 CS_HIDDEN_API void cs_harvest(const CsTables *t, const CsRec *recs, long long n,

@@ -81,6 +81,9 @@ def declare_host_api(lib: C.CDLL) -> C.CDLL:
     """Prototypes of the coherent_search.h host API (ours or the reference's)."""
     P = C.POINTER
     lib.params_defaults.argtypes = [P(SearchParams)]
+    if hasattr(lib, "cs_prep_pad_value"):
+        lib.cs_prep_pad_value.argtypes = [P(C.c_float), C.c_longlong]
+        lib.cs_prep_pad_value.restype = C.c_double
     lib.decimation_set.argtypes = [C.c_int, C.c_int, P(C.c_int), C.c_int]
     lib.decimation_set.restype = C.c_int
     lib.trial_grid_rational.argtypes = [C.c_double, P(C.c_int), P(C.c_int)]
@@ -223,5 +226,5 @@ def candidates_to_numpy(cl: CandidateList) -> np.ndarray:
     n = int(cl.n)
     if n == 0:
         return np.zeros(0, dtype=CAND_DTYPE)
-    buf = C.string_at(C.cast(cl.v, C.c_void_p), n * C.sizeof(Candidate))
-    return np.frombuffer(buf, dtype=CAND_DTYPE).copy()
+    raw = (C.c_char * (n * C.sizeof(Candidate))).from_address(C.cast(cl.v, C.c_void_p).value)
+    return np.frombuffer(raw, dtype=CAND_DTYPE).copy()

@@ -186,9 +186,13 @@ class Session:
     def device_amps_ptr(self) -> int:
         return int(self.gpu.cs_b200_session_device_amps(self.sess))
 
-    def enqueue(self, d_amps_ptr: int | None = None, threshold: float | None = None) -> None:
+    def enqueue(self, d_amps_ptr: int | None = None, threshold: float | None = None,
+                after_stream: int | None = None) -> None:
+        """Queue a search; with `after_stream` (a cudaStream_t handle) it
+        starts after the work already queued there (the spectrum's producer)."""
         thr = self.opts.threshold if threshold is None else threshold
-        rc = self.gpu.cs_b200_session_enqueue_device(self.sess, d_amps_ptr, thr, None)
+        rc = self.gpu.cs_b200_session_enqueue_device(self.sess, d_amps_ptr, thr,
+                                                     after_stream or None)
         if rc != 0:
             raise RuntimeError("enqueue failed")
 

@@ -37,8 +37,10 @@ int cs_b200_session_info(const GpuSession *s, CsB200Info *info);
 float *cs_b200_session_device_amps(GpuSession *s);
 
 /* Enqueue one search of a device-resident spectrum (NULL: the session's own
- * buffer) on the session stream without synchronising.  The kernel is
- * bracketed by CUDA events; cs_b200_session_collect reports its time. */
+ * buffer) on the session stream without synchronising.  A non-NULL `stream`
+ * (a cudaStream_t) is the spectrum's producer: the search starts after the
+ * work queued on it so far.  The kernel is bracketed by CUDA events;
+ * cs_b200_session_collect reports its time. */
 int cs_b200_session_enqueue_device(GpuSession *s, const float *d_amps,
                                    double threshold, void *stream);
 
@@ -107,6 +109,10 @@ int cs_spectrum_run_device(CsSpectrum *s, const float *d_series, float *d_amps, 
 int cs_spectrum_run(CsSpectrum *s, const float *h_series, float *h_amps);
 
 void cs_spectrum_free(CsSpectrum *s);
+
+/* The value prepsubband pads every DM series with: PRESTO's running mean
+ * (update_stats) of DM 0's n output samples.  In libcoherent_search.so. */
+double cs_prep_pad_value(const float *x, long long n);
 
 /* ---- subband dedispersion of 8-bit filterbank data ---------------------
  * The prepsubband stage of the reference's raw-data front end

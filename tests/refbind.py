@@ -27,9 +27,27 @@ def have_ref() -> bool:
     return os.path.exists(os.path.join(REF_DIR, "libcsref.so"))
 
 
+def pin_ref_threads(n: int = 1) -> None:
+    """Run the reference's OpenMP chunk loop (src/search.c:1044-1055) on n
+    threads of the calling thread's team.
+
+    The reference is deterministic only on one thread: each thread's
+    workspace caches a decimated slot's boxcar normalisation and refreshes it
+    when the NUMBER of filled harmonics changes (src/search.c:36-45), while
+    the normalisation depends on WHICH harmonics are filled
+    (src/boxcar.c:170-195).  With chunks dealt round-robin, a thread can go
+    from a low-band chunk (low harmonics missing) to a high-band chunk (top
+    harmonics missing) with the same count and keep the stale shape; with 16
+    threads on a 24576-point, 128 us spectrum this adds 13 candidates in one
+    chunk of the k=3 slot.  On one thread the chunks run in r order and the
+    cache is always current, which is the search's intended result."""
+    C.CDLL("libgomp.so.1").omp_set_num_threads(int(n))
+
+
 def ref_lib() -> C.CDLL:
     global _REF
     if _REF is None:
+        pin_ref_threads(1)
         lib = nt.declare_host_api(C.CDLL(os.path.join(REF_DIR, "libcsref.so")))
         lib.datpipe_create.argtypes = [C.c_int, C.c_int, C.c_double]
         lib.datpipe_create.restype = C.c_void_p

@@ -67,6 +67,65 @@ def test_oracle_matches_reference_live():
     compare_raw(ora[np.argsort(ora["freq"], kind="stable")], ref)
 
 
+def _dedispersed_spectrum(dm: int):
+    """A dedispersed, padded series of the 256-channel front-end case: 24576
+    points at 128 us, so the top harmonics pass Nyquist over most of the band
+    and chunks carry partial harmonic sets at both ends."""
+    from coherentsearch_c_b200.prep import running_mean
+    from test_dedisp import GEOMS, fb_for, ours_tables
+    g = GEOMS["c256_s16_d40"]
+    t = ours_tables(*g)
+    raw = fb_for(g, nblocks=40, seed=11)
+    numout = 24576
+    out = rb.ref_dedisp_run(raw, t.nsub, t.idispdt, t.offsets, t.spectra_per_subint,
+                            t.blocks_per_read, numout)
+    pad = np.float32(running_mean(out[0]))
+    series = np.concatenate([out[dm], np.full(numout - out.shape[1], pad, np.float32)])
+    return rb.ref_spectrum(series, g[7]), numout, g[7]
+
+
+needs_dedisp_ref = pytest.mark.skipif(not (rb.have_ref() and rb.have_dedisp_ref()),
+                                      reason="oracle/_ref not built")
+
+
+@needs_dedisp_ref
+def test_oracle_matches_reference_partial_harmonics():
+    amps, N, dt = _dedispersed_spectrum(25)
+    opts = Options(blocksize=4096, threshold=6.0)
+    ref = rb.ref_search(amps, N, dt, opts, collapse=False)
+    _, _, total, _ = rb.ref_chunks(amps, N, dt, opts)
+    met, geo = rb.oracle_metrics(amps, N, dt, opts, 0, total)
+    ora = rb.oracle_candidates(met, geo, N, dt, opts)
+    compare_raw(ora[np.argsort(ora["freq"], kind="stable")], ref)
+
+
+@needs_dedisp_ref
+def test_reference_threads_change_its_result():
+    """Why the checkers pin the reference to one thread: on 16 threads its
+    per-workspace boxcar-shape cache goes stale in one chunk (trials
+    25815..26276, thread 0's successor of chunk 16) and it reports extra
+    decimated-slot candidates there, all of them outside the one-thread set."""
+    amps, N, dt = _dedispersed_spectrum(25)
+    opts = Options(blocksize=4096, threshold=6.0)
+    one = rb.ref_search(amps, N, dt, opts, collapse=False)
+    try:
+        rb.pin_ref_threads(16)
+        many = rb.ref_search(amps, N, dt, opts, collapse=False)
+    finally:
+        rb.pin_ref_threads(1)
+    r_lo, lodr, _, cstarts = rb.ref_chunks(amps, N, dt, opts)
+    c = int(np.searchsorted(cstarts, 25815))
+    assert cstarts[c] == 25815 and c % 16 == (c - 16) % 16
+    key = lambda a: set(zip(np.round(a["r"], 9), a["nharm"]))
+    extra = key(many) - key(one)
+    assert many.size > one.size and len(extra) == many.size - one.size
+    for r, h in extra:
+        k = opts.nharms // int(h)
+        assert k > 1
+        trial = (r / k - r_lo) / lodr
+        assert cstarts[c] - 0.5 <= trial < cstarts[c + 1] - 0.5
+
+
 @needs_ref
 def test_golden_reference_reproducible():
     """The fixtures are what the reference produces here today."""
