@@ -156,6 +156,44 @@ def cpu_reference_rate(amps, N, seconds=10.0, max_reps=50):
     return total * reps / dt, cores, sample
 
 
+def reference_gpu_rate(amps, N, dt, opts, ours=None, reps=3):
+    """The reference's own GPU form (src/cuda.cu built for sm_100a,
+    oracle/_ref/libcsref_gpu.so) through its search_file on the same
+    spectrum: a session per call (the plain single-file form) and a session
+    kept in its SearchCache (equal-length files).  Host wall time per call,
+    spectrum upload included, like `e2e`."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import refbind as rb
+    if not rb.have_ref_gpu():
+        return {"unavailable": "oracle/_ref/libcsref_gpu.so not built"}
+    _, _, total = opts.geometry(N, dt)
+    rb.ref_search_gpu(amps, N, dt, opts)           # warm: context, cuFFT, pages
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        per_call = rb.ref_search_gpu(amps, N, dt, opts)
+    per_s = (time.perf_counter() - t0) / reps
+    srch = rb.RefGpuSearcher(opts)
+    try:
+        srch.search(amps, N, dt)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            cached = srch.search(amps, N, dt)
+        cached_s = (time.perf_counter() - t0) / reps
+    finally:
+        srch.close()
+    out = {"per_file_trials_per_s": total / per_s, "cached_trials_per_s": total / cached_s,
+           "per_file_ms": 1e3 * per_s, "cached_ms": 1e3 * cached_s,
+           "candidates": int(cached.size),
+           "source": "reference src/cuda.cu (cuFFT c2r) built for sm_100a, called through "
+                     "its search_file with collapse; host wall time per call"}
+    if ours is not None:
+        ka = set(zip(np.round(ours["r"], 9), ours["nharm"]))
+        kb = set(zip(np.round(cached["r"], 9), cached["nharm"]))
+        out["candidates_ours"] = int(ours.size)
+        out["candidates_common"] = len(ka & kb)
+    return out
+
+
 def run_reference(args):
     world, rank, local, pg = dist_setup(args)
     if rank != 0:
@@ -316,6 +354,12 @@ def run_b200(args):
         except Exception as exc:   # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0,
                                     "kind": "reference", "sample": f"unavailable: {exc}"}
+    if rank == 0 and world == 1 and not args.no_ref_gpu:
+        try:
+            line["plain_reference_gpu"] = reference_gpu_rate(amps, N, dt, opts,
+                                                             ours=ses.collapse(out))
+        except Exception as exc:   # noqa: BLE001
+            line["plain_reference_gpu"] = {"unavailable": str(exc)}
     if rank == 0:
         print(json.dumps(line))
     ses.close()
@@ -688,6 +732,32 @@ def _same_cands(a, b):
     return a.size == b.size and all(np.array_equal(a[f], b[f]) for f in ("r", "metric", "nharm"))
 
 
+def sweep_reference_gpu(specs, spectra, dt, opts, trials, ours, batched_ms):
+    """The reference's own GPU form over the same file list, one file at a
+    time through its search_file with one SearchCache (it rebuilds the
+    session whenever the length changes, src/search.c:1388-1406), raw
+    candidates; host wall time."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import refbind as rb
+    if not rb.have_ref_gpu():
+        return {"unavailable": "oracle/_ref/libcsref_gpu.so not built"}
+    srch = rb.RefGpuSearcher(opts)
+    try:
+        srch.search(spectra[0], specs[0].N, dt, collapse=False)     # warm
+        t0 = time.perf_counter()
+        out = [srch.search(a, sp.N, dt, collapse=False) for sp, a in zip(specs, spectra)]
+        wall = time.perf_counter() - t0
+    finally:
+        srch.close()
+    same = sum(1 for x, y in zip(out, ours)
+               if set(zip(np.round(x["r"], 9), x["nharm"])) == set(zip(np.round(y["r"], 9), y["nharm"])))
+    return {"ms": 1e3 * wall, "trials_per_s": trials / wall,
+            "batched_vs_reference_gpu": 1e3 * wall / batched_ms,
+            "files_with_identical_candidate_sets": same, "files": len(specs),
+            "candidates": int(sum(o.size for o in out)),
+            "source": "reference src/cuda.cu built for sm_100a, one SearchCache over the list"}
+
+
 def run_sweep(args):
     """Config 3: 256 files of uneven length searched plain (a session per
     file, the reference's single-file GPU form) and batched (cs_gpu_batch)."""
@@ -746,6 +816,9 @@ def run_sweep(args):
                      "equal_candidates": bool(equal), "differing_files": diff,
                      "candidates": int(sum(o.size for o in res["batched"][1])),
                      "plain_candidates": int(sum(o.size for o in res["plain"][1]))}
+        if not args.no_ref_gpu:
+            lines[nh]["plain_reference_gpu"] = sweep_reference_gpu(
+                specs, spectra, dt, opts, trials, res["batched"][1], res["batched"][0])
     h2d = int(sum(a.nbytes for a in spectra))
     main = lines[60]
     line = {
@@ -875,6 +948,8 @@ def main():
     ap.add_argument("--pool", type=int, default=48, help="serve: distinct spectra")
     ap.add_argument("--mem-budget-gb", type=int, default=24, help="serve: device budget")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip the reference's own GPU form (plain single-file baseline)")
     ap.add_argument("--nspec-log2", type=int, default=0,
                     help="dedisp workload length 2^n spectra (default: the 2^22 workload; "
                          "smaller sizes are for profiling captures only)")

@@ -4,6 +4,8 @@
                      unmodified by oracle/Makefile against the FFTW-API shim)
 * libcsoracle.so  -- oracle/cs_oracle.c, the per-trial CPU restatement
 * libdedisp_ref.so -- the reference's vendored PRESTO dispersion.c
+* libcsref_gpu.so  -- the reference's search path on its own src/cuda.cu
+                     backend for sm_100a (the plain GPU form)
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use these.
 """
@@ -58,6 +60,71 @@ def ref_lib() -> C.CDLL:
         lib.search_cache_free.argtypes = [C.c_void_p]
         _REF = lib
     return _REF
+
+
+def have_ref_gpu() -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "libcsref_gpu.so"))
+
+
+_REF_GPU = None
+
+
+def ref_gpu_lib() -> C.CDLL:
+    """The reference's search path with its own src/cuda.cu backend (the
+    plain single-file GPU form), built by `make -C oracle refgpu`."""
+    global _REF_GPU
+    if _REF_GPU is None:
+        ref_lib()                       # pins the OpenMP team before the load
+        _REF_GPU = nt.declare_host_api(C.CDLL(os.path.join(REF_DIR, "libcsref_gpu.so")))
+    return _REF_GPU
+
+
+def ref_search_gpu(amps: np.ndarray, N: int, dt: float, opts, device: int = 0,
+                   collapse: bool = True) -> np.ndarray:
+    """The reference's search_file (src/search.c:1247) on its own GPU backend
+    (src/search.c:1374-1406 -> src/cuda.cu), one session per call."""
+    lib = ref_gpu_lib()
+    ft = make_file(amps, N, dt)
+    p = opts.params(lib)
+    rem = int(opts.remove) if collapse else 0
+    hrem = int(opts.harm_remove) if collapse else 0
+    cl = lib.search_file(C.byref(ft), C.byref(p), opts.lofreq, opts.hifreq, opts.lobin,
+                         opts.blocksize, opts.threshold, rem, opts.drtol, hrem, opts.numharm,
+                         None, 0, 0, 0, None, None, 1.0, int(device))
+    out = nt.candidates_to_numpy(cl)
+    lib.candlist_free(C.byref(cl))
+    return out
+
+
+class RefGpuSearcher:
+    """The reference's GPU form with its SearchCache kept across calls (the
+    session is reused while the geometry matches, src/search.c:1388-1406), as
+    its list driver runs a sweep of equal-length files (src/cli.c:976)."""
+
+    def __init__(self, opts, device: int = 0):
+        self.lib = ref_gpu_lib()
+        self.lib.search_cache_free.argtypes = [C.c_void_p]
+        self.opts = opts
+        self.device = device
+        self.p = opts.params(self.lib)           # one address: part of the session match
+        self.cache = C.create_string_buffer(8192)  # zeroed, as the CLI memsets it
+
+    def search(self, amps: np.ndarray, N: int, dt: float, collapse: bool = True):
+        o = self.opts
+        ft = make_file(amps, N, dt)
+        cl = self.lib.search_file(C.byref(ft), C.byref(self.p), o.lofreq, o.hifreq, o.lobin,
+                                  o.blocksize, o.threshold, int(o.remove) if collapse else 0,
+                                  o.drtol, int(o.harm_remove) if collapse else 0, o.numharm,
+                                  None, 0, 0, 0, None, C.addressof(self.cache), 1.0,
+                                  int(self.device))
+        out = nt.candidates_to_numpy(cl)
+        self.lib.candlist_free(C.byref(cl))
+        return out
+
+    def close(self) -> None:
+        if self.cache is not None:
+            self.lib.search_cache_free(C.addressof(self.cache))
+            self.cache = None
 
 
 def oracle_lib() -> C.CDLL:

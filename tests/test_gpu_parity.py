@@ -85,6 +85,27 @@ def test_candidates_vs_reference_small(gpu_ready):
     ses.close()
 
 
+@pytest.mark.skipif(not rb.have_ref_gpu(), reason="oracle/_ref/libcsref_gpu.so not built")
+@pytest.mark.parametrize("nharms", [60, 32])
+def test_reference_gpu_form_agrees(gpu_ready, nharms):
+    """The reference's own GPU backend (src/cuda.cu, cuFFT c2r) on the same
+    spectrum: the same candidates, S/N within the f32 tolerance, and the same
+    order once ours goes through search_file's frequency sort
+    (src/search.c:1467-1478 sorts even without collapsing)."""
+    spec, amps = _small_case()
+    opts = Options(nharms=nharms, blocksize=2048, threshold=6.0)
+    ref = rb.ref_search_gpu(amps, spec.N, spec.dt, opts, collapse=False)
+    ses = Session(spec.N, spec.dt, opts)
+    raw = ses.run_raw(amps)
+    ses.close()
+    assert ref.size > 100
+    got = raw[np.argsort(raw["freq"], kind="stable")]
+    only_ours, only_ref = match_candidates(got, ref, 6.0, SNR_RTOL_F32)
+    if not only_ours and not only_ref:
+        np.testing.assert_array_equal(got["r"], ref["r"])
+        np.testing.assert_array_equal(got["nharm"], ref["nharm"])
+
+
 GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
 
 
