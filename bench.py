@@ -901,8 +901,34 @@ def run_serve(args):
         "gpu_launches": 2 * len(reqs),
         "clocks": clk.summary(),
     }
+    if not args.no_ref_gpu:
+        line["plain_reference_gpu"] = serve_reference_gpu(reqs, served["results"],
+                                                          served["trials_per_s"])
     print(json.dumps(line))
     return 0
+
+
+def serve_reference_gpu(reqs, served_results, served_rate, limit=60):
+    """The reference's own GPU form serving the first `limit` requests back to
+    back (no arrival gaps, so it is not idle): its search_file with a session
+    per request, raw candidates; host wall time."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import refbind as rb
+    if not rb.have_ref_gpu():
+        return {"unavailable": "oracle/_ref/libcsref_gpu.so not built"}
+    sub = reqs[:limit]
+    rb.ref_search_gpu(sub[0].amps, sub[0].N, sub[0].dt, sub[0].opts, collapse=False)  # warm
+    t0 = time.perf_counter()
+    out = [rb.ref_search_gpu(r.amps, r.N, r.dt, r.opts, collapse=False) for r in sub]
+    wall = time.perf_counter() - t0
+    trials = sum(r.trials for r in sub)
+    same = sum(1 for x, y in zip(out, served_results)
+               if set(zip(np.round(x["r"], 9), x["nharm"])) == set(zip(np.round(y["r"], 9), y["nharm"])))
+    return {"requests": len(sub), "trials_per_s": trials / wall, "mean_ms": 1e3 * wall / len(sub),
+            "served_vs_reference_gpu": served_rate / (trials / wall),
+            "requests_with_identical_candidate_sets": same,
+            "source": "reference src/cuda.cu built for sm_100a, search_file per request, "
+                      "requests back to back (a lower bound on its latency under load)"}
 
 
 def profiled_traffic(kernel, total):
