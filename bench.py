@@ -156,6 +156,38 @@ def cpu_reference_rate(amps, N, seconds=10.0, max_reps=50):
     return total * reps / dt, cores, sample
 
 
+def ducy_timing(ses, cands, amps, N, dt, reps=3):
+    """Duty cycles (measure_ducy) of the step's raw candidates: on the GPU
+    from the session's resident spectrum, and by the reference's own host
+    code (oracle/_ref/libcsref.so) on the same list; equal widths checked."""
+    import ctypes as C
+    from coherentsearch_c_b200 import native as nt
+    from coherentsearch_c_b200.search import Options
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import refbind as rb
+    ses.measure_ducy(cands[:8])                       # plan + tables
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        got = ses.measure_ducy(cands)["ducy"]
+    gpu_ms = 1e3 * (time.perf_counter() - t0) / reps
+    lib = rb.ref_lib()
+    ft = rb.make_file(amps, N, dt)
+    p = Options().params(lib)
+    buf = (nt.Candidate * max(cands.size, 1))()
+    C.memmove(buf, cands.ctypes.data, cands.size * C.sizeof(nt.Candidate))
+    cl = nt.CandidateList(C.cast(buf, C.POINTER(nt.Candidate)), cands.size, cands.size)
+    t0 = time.perf_counter()
+    res = lib.measure_ducy(C.byref(ft), C.byref(cl), C.byref(p))
+    host_ms = 1e3 * (time.perf_counter() - t0)
+    ref = nt.candidates_to_numpy(res)["ducy"]
+    lib.candlist_free(C.byref(res))
+    return {"candidates": int(cands.size), "gpu_ms": gpu_ms, "reference_host_ms": host_ms,
+            "equal": bool(np.array_equal(got, ref, equal_nan=True)),
+            "note": "GPU: cs_ducy_run_device on the session's resident spectrum, host wall "
+                    "time with the candidate upload and result readback; reference: its "
+                    "measure_ducy on one host thread"}
+
+
 def reference_gpu_rate(amps, N, dt, opts, ours=None, reps=3):
     """The reference's own GPU form (src/cuda.cu built for sm_100a,
     oracle/_ref/libcsref_gpu.so) through its search_file on the same
@@ -354,6 +386,11 @@ def run_b200(args):
         except Exception as exc:   # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0,
                                     "kind": "reference", "sample": f"unavailable: {exc}"}
+    if rank == 0 and world == 1:
+        try:
+            line["ducy"] = ducy_timing(ses, out, amps, N, dt)
+        except Exception as exc:   # noqa: BLE001
+            line["ducy"] = {"unavailable": str(exc)}
     if rank == 0 and world == 1 and not args.no_ref_gpu:
         try:
             line["plain_reference_gpu"] = reference_gpu_rate(amps, N, dt, opts,

@@ -33,7 +33,7 @@ CFLAGS = ["-O2", "-fPIC", "-std=gnu11", "-ffp-contract=off", "-Wall", "-Wextra",
 HOST_COMMON = ["cs_common.c"]
 HOST_GPU_ONLY = ["cs_tables.c"]
 HOST_LIB = ["cs_common.c", "cs_search.c"]
-CUDA_SRCS = ["cs_gpu.cu", "cs_dedisp.cu", "cs_spectrum.cu"]
+CUDA_SRCS = ["cs_gpu.cu", "cs_dedisp.cu", "cs_spectrum.cu", "cs_ducy.cu"]
 
 
 def _run(cmd, verbose):

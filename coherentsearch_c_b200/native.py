@@ -173,6 +173,12 @@ def declare_gpu_api(lib: C.CDLL) -> C.CDLL:
     lib.cs_spectrum_run.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     lib.cs_spectrum_run.restype = C.c_int
     lib.cs_spectrum_free.argtypes = [C.c_void_p]
+    lib.cs_ducy_create.argtypes = [C.c_double, C.c_double, C.c_int]
+    lib.cs_ducy_create.restype = C.c_void_p
+    lib.cs_ducy_run_device.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_longlong,
+                                       C.c_void_p, C.c_longlong, P(C.c_double), C.c_void_p]
+    lib.cs_ducy_run_device.restype = C.c_int
+    lib.cs_ducy_free.argtypes = [C.c_void_p]
     IP = P(C.c_int)
     lib.cs_dedisp_tables.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                      C.c_double, C.c_double, C.c_double, C.c_int, IP, IP, IP,

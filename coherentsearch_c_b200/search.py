@@ -183,6 +183,27 @@ class Session:
         self.host.candlist_free(C.byref(cl))
         return out
 
+    def measure_ducy(self, cands: np.ndarray) -> np.ndarray:
+        """measure_ducy (src/candidate.c:305-329) on the GPU against the
+        spectrum this session last searched (still in device memory): a copy
+        of `cands` with the ducy field filled in."""
+        out = np.array(cands, dtype=nt.CAND_DTYPE, copy=True)
+        if out.size == 0:
+            return out
+        if getattr(self, "_ducy", None) is None:
+            self._ducy = self.gpu.cs_ducy_create(self.params.boxcar_fsp,
+                                                  self.params.boxcar_maxfrac, self.device)
+            if not self._ducy:
+                raise RuntimeError("cs_ducy_create failed (see stderr)")
+        d = np.empty(out.size, dtype=np.float64)
+        rc = self.gpu.cs_ducy_run_device(self._ducy, self.device_amps_ptr(), self.namps, self.N,
+                                         out.ctypes.data, out.size,
+                                         d.ctypes.data_as(C.POINTER(C.c_double)), None)
+        if rc != 0:
+            raise RuntimeError("cs_ducy_run_device failed (see stderr)")
+        out["ducy"] = d
+        return out
+
     def device_amps_ptr(self) -> int:
         return int(self.gpu.cs_b200_session_device_amps(self.sess))
 
@@ -208,6 +229,9 @@ class Session:
         return out, ms.value, rc
 
     def close(self) -> None:
+        if getattr(self, "_ducy", None):
+            self.gpu.cs_ducy_free(self._ducy)
+            self._ducy = None
         if getattr(self, "sess", None):
             self.gpu.cs_gpu_session_free(self.sess)
             self.sess = None

@@ -110,6 +110,20 @@ int cs_spectrum_run(CsSpectrum *s, const float *h_series, float *h_amps);
 
 void cs_spectrum_free(CsSpectrum *s);
 
+/* ---- duty cycles on the device ------------------------------------------
+ * measure_ducy (src/candidate.c:305-329) for candidates of a spectrum that is
+ * already in device memory (a session's buffer, cs_b200_session_device_amps):
+ * the m = 64 FP64 profile of each candidate's harmonics, its boxcar widths
+ * for the search's fsp / maxfrac, and width / bins of the best one.
+ * ducy_out[i] is NaN where measure_ducy leaves it NaN (nharm < 1, r <= 0;
+ * also nharm > 64).  Returns 0, or -1 on error. */
+typedef struct CsDucy CsDucy;
+CsDucy *cs_ducy_create(double fsp, double maxfrac, int device);
+int cs_ducy_run_device(CsDucy *d, const float *d_amps, long long namps, long long N,
+                       const Candidate *cands, long long ncand, double *ducy_out,
+                       void *stream);
+void cs_ducy_free(CsDucy *d);
+
 /* The value prepsubband pads every DM series with: PRESTO's running mean
  * (update_stats) of DM 0's n output samples.  In libcoherent_search.so. */
 double cs_prep_pad_value(const float *x, long long n);
