@@ -33,7 +33,11 @@ CFLAGS = ["-O2", "-fPIC", "-std=gnu11", "-ffp-contract=off", "-Wall", "-Wextra",
 HOST_COMMON = ["cs_common.c"]
 HOST_GPU_ONLY = ["cs_tables.c"]
 HOST_LIB = ["cs_common.c", "cs_search.c"]
-CUDA_SRCS = ["cs_gpu.cu", "cs_dedisp.cu", "cs_spectrum.cu", "cs_ducy.cu"]
+CUDA_SRCS = ["cs_gpu.cu", "cs_dedisp.cu", "cs_spectrum.cu", "cs_ducy.cu",
+             "cs_collapse.cu"]
+# FP64 candidate arithmetic that must round like the host restatements, which
+# are built with -ffp-contract=off: no multiply-add contraction
+CUDA_FLAGS = {"cs_ducy.cu": ["-fmad=false"], "cs_collapse.cu": ["-fmad=false"]}
 
 
 def _run(cmd, verbose):
@@ -80,8 +84,8 @@ def build(verbose: bool = False, force: bool = False) -> None:
         o = os.path.join(OBJ, src.replace(".cu", ".o"))
         if force or _newer(o, [s] + hdrs):
             _run([NVCC] + GENCODE + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler",
-                  "-fPIC,-fvisibility=hidden", f"-I{INC}", f"-I{CSRC}", "-c", s, "-o", o],
-                 verbose)
+                  "-fPIC,-fvisibility=hidden", f"-I{INC}", f"-I{CSRC}"] +
+                 CUDA_FLAGS.get(src, []) + ["-c", s, "-o", o], verbose)
         gpu_objs.append(o)
     libgpu = os.path.join(LIB, "libcsgpu.so")
     if force or _newer(libgpu, gpu_objs):

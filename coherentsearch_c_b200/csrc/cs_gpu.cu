@@ -605,6 +605,7 @@ cs_search_kernel(const SearchArgs args)
 }
 
 #include "cs_search_ws.cuh"
+#include "cs_collapse.h"
 
 /* ------------------------------------------------------------------ */
 /* Host side                                                          */
@@ -650,6 +651,7 @@ struct GpuSession {
     unsigned cap;
     unsigned *h_count;     /* pinned */
     CsRec *h_recs;         /* pinned record staging, grown on demand */
+    CsCollapse *coll;      /* device harvest + collapse scratch, on first use */
     size_t h_recs_cap;
     float last_kernel_ms;
     int own_plans;
@@ -729,6 +731,7 @@ static void session_release(GpuSession *S)
     cudaFree(S->d_harm2);
     if (S->h_count) cudaFreeHost(S->h_count);
     if (S->h_recs) cudaFreeHost(S->h_recs);
+    cs_collapse_free(S->coll);
     if (S->ev0) cudaEventDestroy(S->ev0);
     if (S->ev1) cudaEventDestroy(S->ev1);
     if (S->ev_in) cudaEventDestroy(S->ev_in);
@@ -1279,6 +1282,48 @@ CS_EXPORT int cs_b200_session_collect(GpuSession *S, double threshold, Candidate
         *kernel_ms = ms;
     }
     return rerun ? 1 : 0;
+}
+
+CS_EXPORT int cs_b200_session_collect_collapsed(GpuSession *S, double threshold, int remove,
+                                                double dr_tol, int harm_remove, int numharm,
+                                                double harm_tol, CandidateList *out,
+                                                float *kernel_ms)
+{
+    if (!S || !out) return -1;
+    candlist_init(out);
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(S->h_count, S->d_count, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                             S->st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(S->h_count + 1, S->d_err, sizeof(int), cudaMemcpyDeviceToHost,
+                             S->st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(S->st)) != cudaSuccess) {
+        fprintf(stderr, "Error: B200 search failed: %s\n", cudaGetErrorString(e));
+        return -1;
+    }
+    if (S->h_count[1] != 0) {
+        fprintf(stderr, "Error: B200 search kernel timed out waiting for the tensor cores\n");
+        return -1;
+    }
+    if (kernel_ms) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, S->ev0, S->ev1);
+        *kernel_ms = ms;
+    }
+    const unsigned n = S->h_count[0];
+    if (n > S->cap) {
+        if (grow_records(S, n + n / 8 + 1024) != 0) return -1;
+        return 1;
+    }
+    if (!S->coll && !(S->coll = cs_collapse_new())) return -1;
+    int k[CS_MAX_SLOT], Hk[CS_MAX_SLOT];
+    for (int i = 0; i < S->tab.nslot; i++) {
+        k[i] = S->tab.slot[i].k;
+        Hk[i] = S->tab.slot[i].Hk;
+    }
+    return cs_collapse_run(S->coll, S->d_recs, n, S->d_chunks, S->tab.nchunks, k, Hk,
+                           S->tab.nslot, S->Nprof, S->r_lo, S->lodr, (double)S->N, S->T,
+                           threshold, remove, dr_tol, harm_remove, numharm, harm_tol, S->st,
+                           out) == 0 ? 0 : -1;
 }
 
 CS_EXPORT float *cs_b200_session_device_amps(GpuSession *S)

@@ -148,6 +148,10 @@ def declare_gpu_api(lib: C.CDLL) -> C.CDLL:
     lib.cs_b200_session_collect.argtypes = [C.c_void_p, C.c_double, P(CandidateList),
                                             P(C.c_float)]
     lib.cs_b200_session_collect.restype = C.c_int
+    lib.cs_b200_session_collect_collapsed.argtypes = [C.c_void_p, C.c_double, C.c_int,
+                                                      C.c_double, C.c_int, C.c_int, C.c_double,
+                                                      P(CandidateList), P(C.c_float)]
+    lib.cs_b200_session_collect_collapsed.restype = C.c_int
     lib.cs_b200_session_sync.argtypes = [C.c_void_p]
     lib.cs_b200_session_sync.restype = C.c_int
     lib.cs_b200_session_search_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_double,

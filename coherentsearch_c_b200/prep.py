@@ -78,11 +78,12 @@ class PrepSearch:
         self.spec.run_device(self.out[d].data_ptr(), ses.device_amps_ptr(),
                              self.stream.cuda_stream)
 
-    def _finish(self, ses: Session, threshold: float | None) -> np.ndarray:
-        out, ms, rc = ses.collect(threshold)
+    def _finish(self, ses: Session, threshold: float | None, collapse: bool = False) -> np.ndarray:
+        get = ses.collect_collapsed if collapse else ses.collect
+        out, ms, rc = get(threshold)
         if rc == 1:                     # record buffer grown: run again
             ses.enqueue(None, threshold)
-            out, ms, rc = ses.collect(threshold)
+            out, ms, rc = get(threshold)
         self.search_ms.append(ms)
         return out
 
@@ -93,9 +94,11 @@ class PrepSearch:
         ses.enqueue(None, threshold, after_stream=self.stream.cuda_stream)
         return self._finish(ses, threshold)
 
-    def search_all(self, threshold: float | None = None, dms=None) -> list[np.ndarray]:
-        """Raw candidates of every DM (or of `dms`), pipelined over the two
-        sessions; results in DM order."""
+    def search_all(self, threshold: float | None = None, dms=None,
+                   collapse: bool = False) -> list[np.ndarray]:
+        """Candidates of every DM (or of `dms`), pipelined over the two
+        sessions, in DM order: raw, or with `collapse` the list search_file
+        returns, collapsed on the GPU."""
         dms = list(range(self.t.ndm)) if dms is None else list(dms)
         res: list[np.ndarray] = []
         self.search_ms = []
@@ -105,17 +108,16 @@ class PrepSearch:
             self._spectrum(d, ses)
             ses.enqueue(None, threshold, after_stream=self.stream.cuda_stream)
             if i > 0:
-                res.append(self._finish(self.sessions[(i - 1) & 1], threshold))
+                res.append(self._finish(self.sessions[(i - 1) & 1], threshold, collapse))
         if dms:
-            res.append(self._finish(self.sessions[(len(dms) - 1) & 1], threshold))
+            res.append(self._finish(self.sessions[(len(dms) - 1) & 1], threshold, collapse))
         return res
 
     def run(self, d_raw: int, nspec: int, collapse: bool = True) -> list[np.ndarray]:
         """Candidates of every DM, in DM order (collapsed as search_file does
         unless collapse is False)."""
         self.dedisperse(d_raw, nspec)
-        raw = self.search_all()
-        return [self.ses.collapse(r) for r in raw] if collapse else raw
+        return self.search_all(collapse=collapse)
 
     def series(self, d: int) -> np.ndarray:
         self.stream.synchronize()

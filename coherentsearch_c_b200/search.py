@@ -163,25 +163,47 @@ class Session:
         return out
 
     def collapse(self, raw: np.ndarray) -> np.ndarray:
-        """The post-processing of search_file (src/search.c:1467-1478)."""
-        n = raw.size
-        buf = (nt.Candidate * max(n, 1))()
-        if n:
-            C.memmove(buf, raw.ctypes.data, n * C.sizeof(nt.Candidate))
-        cl = nt.CandidateList(C.cast(buf, C.POINTER(nt.Candidate)), n, n)
+        """The post-processing of search_file (src/search.c:1467-1478) on the
+        host: remove_duplicates when `remove`, else a stable frequency sort;
+        then remove_harmonics when `harm_remove`."""
         if self.opts.remove:
+            n = raw.size
+            buf = (nt.Candidate * max(n, 1))()
+            if n:
+                C.memmove(buf, raw.ctypes.data, n * C.sizeof(nt.Candidate))
+            cl = nt.CandidateList(C.cast(buf, C.POINTER(nt.Candidate)), n, n)
             cl = self.host.remove_duplicates(C.byref(cl), self.opts.drtol)
-        else:
-            arr = raw.copy()
-            idx = np.argsort(arr["freq"], kind="stable")
-            return arr[idx]
-        if self.opts.harm_remove:
-            cl2 = self.host.remove_harmonics(C.byref(cl), self.opts.numharm, 1.0)
+            arr = nt.candidates_to_numpy(cl)
             self.host.candlist_free(C.byref(cl))
-            cl = cl2
+        else:
+            arr = raw[np.argsort(raw["freq"], kind="stable")]
+        if self.opts.harm_remove:
+            n = arr.size
+            buf = (nt.Candidate * max(n, 1))()
+            if n:
+                C.memmove(buf, np.ascontiguousarray(arr).ctypes.data, n * C.sizeof(nt.Candidate))
+            cl = nt.CandidateList(C.cast(buf, C.POINTER(nt.Candidate)), n, n)
+            cl2 = self.host.remove_harmonics(C.byref(cl), self.opts.numharm, 1.0)
+            arr = nt.candidates_to_numpy(cl2)
+            self.host.candlist_free(C.byref(cl2))
+        return arr
+
+    def collect_collapsed(self, threshold: float | None = None):
+        """cs_b200_session_collect_collapsed: the enqueued search's candidates
+        harvested and collapsed on the GPU (the records stay on the device).
+        Returns (candidates, kernel ms, rc) like collect."""
+        thr = self.opts.threshold if threshold is None else threshold
+        cl = nt.CandidateList()
+        ms = C.c_float(0)
+        o = self.opts
+        rc = self.gpu.cs_b200_session_collect_collapsed(self.sess, thr, int(o.remove), o.drtol,
+                                                        int(o.harm_remove), o.numharm, 1.0,
+                                                        C.byref(cl), C.byref(ms))
+        if rc < 0:
+            raise RuntimeError("collect_collapsed failed")
         out = nt.candidates_to_numpy(cl)
         self.host.candlist_free(C.byref(cl))
-        return out
+        return out, ms.value, rc
 
     def measure_ducy(self, cands: np.ndarray) -> np.ndarray:
         """measure_ducy (src/candidate.c:305-329) on the GPU against the

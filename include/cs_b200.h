@@ -52,6 +52,17 @@ int cs_b200_session_collect(GpuSession *s, double threshold, CandidateList *out,
 
 int cs_b200_session_sync(GpuSession *s);
 
+/* Like cs_b200_session_collect, but the records never leave the device: they
+ * are harvested, ordered and collapsed there exactly as search_file's
+ * post-processing does (src/search.c:1467-1478: remove_duplicates with
+ * dr_tol when `remove`, else a stable frequency sort; then remove_harmonics
+ * with numharm / harm_tol when `harm_remove`), and only the resulting list
+ * comes back.  Returns 0, 1 if the record buffer overflowed (grown; enqueue
+ * again), or -1. */
+int cs_b200_session_collect_collapsed(GpuSession *s, double threshold, int remove,
+                                      double dr_tol, int harm_remove, int numharm,
+                                      double harm_tol, CandidateList *out, float *kernel_ms);
+
 /* ---- batched search of many spectra -------------------------------------
  * No reference counterpart: the reference searches one file per call
  * (src/search.c:1388-1406) and rebuilds its GPU session whenever the file

@@ -53,3 +53,10 @@ def test_prep_search_matches_reference(gpu_ready):
             if d == 25:   # search_file's post-processing on top
                 refc = rb.ref_search(amps, numout, dt, opts, collapse=True)
                 match_candidates(ps.ses.collapse(got), refc, opts.threshold, SNR_RTOL_F32)
+        # the same loop collapsing on the GPU: the host collapse of the raw lists
+        collapsed = ps.search_all(collapse=True)
+        for d in range(t.ndm):
+            host = ps.ses.collapse(every[d])
+            assert collapsed[d].size == host.size
+            for f in ("freq", "metric", "r", "nharm"):
+                np.testing.assert_array_equal(collapsed[d][f], host[f])
