@@ -634,7 +634,7 @@ def run_prep(args):
 
     def step():
         ps.dedisperse(raw.data_ptr(), spec.nspec)
-        return ps.search_all()
+        return ps.search_all(collapse=True)      # search_file's list per DM
 
     for _ in range(args.warmup):
         step()
@@ -675,7 +675,9 @@ def run_prep(args):
         "data": "synthetic",
         "config": dict(workload=W["workload"] + "; search of every DM: N=" + str(N)
                        + " (numout), nharms 60, m 16, hidr 0.5, 0.1-125 Hz, maxdecim 6, "
-                       "blocksize 65536, threshold 8", ndm=t.ndm, trials_per_dm=total,
+                       "blocksize 65536, threshold 8; each DM's candidates collapsed "
+                       "(remove_duplicates + remove_harmonics) on the GPU",
+                       ndm=t.ndm, trials_per_dm=total,
                        output_per_dm=ps.nout,
                        l2="inputs larger than L2 (raw input and dedispersed output > 126 MB)",
                        parallelism=f"replicas{world}"),
