@@ -98,13 +98,14 @@ __global__ void gather_bits_kernel(const unsigned *order, const double *v, unsig
     if (i < n) bits[i] = (uint64_t)__double_as_longlong(v[order[i]]);
 }
 
-/* run starts of remove_duplicates over the first nv of the r-sorted list */
-__global__ void run_flags_kernel(const unsigned *order, const double *r, const unsigned *nv,
-                                 double drtol, unsigned *flag)
+/* run starts of remove_duplicates over the first nv of the r-sorted list
+ * (zero past nv, so that a scan over all n entries counts only real runs) */
+__global__ void run_flags_kernel(const unsigned *order, const double *r, unsigned n,
+                                 const unsigned *nv, double drtol, unsigned *flag)
 {
     const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= *nv) return;
-    flag[i] = (i == 0 || r[order[i]] - r[order[i - 1]] > drtol) ? 1u : 0u;
+    if (i >= n) return;
+    flag[i] = i < *nv && (i == 0 || r[order[i]] - r[order[i - 1]] > drtol) ? 1u : 0u;
 }
 
 /* each run start scans its run: the first member of largest metric */
@@ -124,19 +125,24 @@ __global__ void run_pick_kernel(const unsigned *order, const double *metric,
     out[runid[i]] = best;
 }
 
-__global__ void count_runs_kernel(const unsigned *flag, const unsigned *runid,
-                                  const unsigned *nv, unsigned *m)
+__global__ void count_runs_kernel(const unsigned *flag, const unsigned *runid, unsigned n,
+                                  unsigned *m)
 {
-    const unsigned n = *nv;
-    *m = n ? runid[n - 1] + flag[n - 1] : 0u;
+    *m = runid[n - 1] + flag[n - 1];
 }
 
-__global__ void gather_metric_kernel(const unsigned *list, const double *metric, unsigned m,
-                                     double *key, unsigned *pos)
+__global__ void copy_count_kernel(const unsigned *src, unsigned *dst)
+{
+    *dst = *src;
+}
+
+/* descending-sort keys; entries past m sort after every real one */
+__global__ void gather_metric_kernel(const unsigned *list, const double *metric, unsigned n,
+                                     const unsigned *m, double *key, unsigned *pos)
 {
     const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m) return;
-    key[i] = metric[list[i]];
+    if (i >= n) return;
+    key[i] = i < *m ? metric[list[i]] : -INFINITY;
     pos[i] = i;
 }
 
@@ -155,10 +161,12 @@ static __device__ bool related(double r1, double r2, int numharm, double tol)
 
 /* remove_harmonics' greedy loop over the metric-ordered list (one CTA) */
 __global__ void __launch_bounds__(1024) greedy_kernel(const unsigned *list, const unsigned *pos,
-                                                      const double *r, unsigned m, int numharm,
-                                                      double tol, unsigned char *removed,
+                                                      const double *r, const unsigned *mp,
+                                                      int numharm, double tol,
+                                                      unsigned char *removed,
                                                       unsigned char *keep_by_pos)
 {
+    const unsigned m = *mp;
     for (unsigned j = threadIdx.x; j < m; j += blockDim.x) removed[j] = 0;
     __syncthreads();
     for (unsigned i = 0; i < m; i++) {
@@ -171,10 +179,11 @@ __global__ void __launch_bounds__(1024) greedy_kernel(const unsigned *list, cons
     for (unsigned q = threadIdx.x; q < m; q += blockDim.x) keep_by_pos[pos[q]] = !removed[q];
 }
 
-__global__ void emit_kernel(const unsigned *list, const unsigned char *keep, unsigned m,
+__global__ void emit_kernel(const unsigned *list, const unsigned char *keep, const unsigned *mp,
                             const double *r, const double *freq, const double *metric,
                             const int *nharm, Candidate *out, unsigned *nout)
 {
+    const unsigned m = *mp;
     /* one CTA: an ordered compaction (m is a few thousand at most) */
     __shared__ unsigned base;
     __shared__ unsigned warp_tot[32];
@@ -229,6 +238,7 @@ struct CsCollapse {
     size_t h_out_cap;
     void *temp;
     size_t temp_bytes;
+    unsigned pending_n;             /* records of the enqueued collapse */
 };
 
 static void collapse_release_buffers(CsCollapse *w)
@@ -320,14 +330,14 @@ static int bit_length_u64(uint64_t v)
     return b;
 }
 
-int cs_collapse_run(CsCollapse *w, const CsRec *recs, unsigned n, const CsChunk *chunks,
-                    long long nchunks, const int *slot_k, const int *slot_Hk, int nslot,
-                    int nprof, double r_lo, double lodr, double N, double T, double threshold,
-                    int remove, double dr_tol, int harm_remove, int numharm, double harm_tol,
-                    cudaStream_t st, CandidateList *out)
+int cs_collapse_enqueue(CsCollapse *w, const CsRec *recs, unsigned n, const CsChunk *chunks,
+                        long long nchunks, const int *slot_k, const int *slot_Hk, int nslot,
+                        int nprof, double r_lo, double lodr, double N, double T,
+                        double threshold, int remove, double dr_tol, int harm_remove,
+                        int numharm, double harm_tol, cudaStream_t st)
 {
-    candlist_init(out);
     if (!w || nslot < 1 || nslot > CS_MAX_SLOT || nprof < 1 || nchunks < 1) return -1;
+    w->pending_n = n;
     if (n == 0) return 0;
     cl::SlotInfo si;
     memset(&si, 0, sizeof(si));
@@ -335,16 +345,19 @@ int cs_collapse_run(CsCollapse *w, const CsRec *recs, unsigned n, const CsChunk 
     const unsigned g = (n + cl::NT - 1) / cl::NT;
     const int end_bit = bit_length_u64((uint64_t)nchunks * (uint64_t)nslot * (uint64_t)nprof);
     size_t tb = 0;
-    unsigned nv = 0, mlen = 0, nout = 0;
     const unsigned *order = nullptr, *listp = nullptr;
     const unsigned char *keep = nullptr;
-    cudaError_t e = collapse_reserve(w, n);
-    if (e == cudaSuccess) e = cudaMemsetAsync(w->counters, 0, 4 * sizeof(unsigned), st);
+    cudaError_t e = collapse_reserve(w, n);       /* allocates the counters on first use */
+    if (e != cudaSuccess || !w->counters) {
+        fprintf(stderr, "Error: candidate collapse on the GPU: %s\n", cudaGetErrorString(e));
+        return -1;
+    }
+    unsigned *nv = w->counters, *m = w->counters + 1, *nout = w->counters + 2;
+    e = cudaMemsetAsync(w->counters, 0, 4 * sizeof(unsigned), st);
     if (e == cudaSuccess) {
         cl::harvest_kernel<<<g, cl::NT, 0, st>>>(recs, n, chunks, si, nslot, nprof, r_lo, lodr,
                                                  N / 2.0, T, threshold, w->key[0], w->idx[0],
-                                                 w->r, w->freq, w->metric, w->nharm,
-                                                 w->counters);
+                                                 w->r, w->freq, w->metric, w->nharm, nv);
         e = cudaGetLastError();
     }
     /* the base order: (chunk, slot, j); invalid records (all-ones key) last */
@@ -366,89 +379,95 @@ int cs_collapse_run(CsCollapse *w, const CsRec *recs, unsigned n, const CsChunk 
         tb = w->temp_bytes;
         e = cub::DeviceRadixSort::SortPairs(w->temp, tb, kb2, ib2, (int)n, 0, 64, st);
     }
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(w->h_counters, w->counters, sizeof(unsigned), cudaMemcpyDeviceToHost,
-                            st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) goto fail;
-    nv = w->h_counters[0];
-    if (nv == 0) return 0;
     order = ib2.Current();
     if (remove) {
-        const unsigned gv = (nv + cl::NT - 1) / cl::NT;
-        cl::run_flags_kernel<<<gv, cl::NT, 0, st>>>(order, w->r, w->counters, dr_tol, w->flag);
-        e = cudaGetLastError();
         if (e == cudaSuccess) {
-            tb = w->temp_bytes;
-            e = cub::DeviceScan::ExclusiveSum(w->temp, tb, w->flag, w->runid, (int)nv, st);
-        }
-        if (e == cudaSuccess) {
-            cl::run_pick_kernel<<<gv, cl::NT, 0, st>>>(order, w->metric, w->flag, w->runid,
-                                                       w->counters, w->list);
-            cl::count_runs_kernel<<<1, 1, 0, st>>>(w->flag, w->runid, w->counters,
-                                                   w->counters + 1);
+            cl::run_flags_kernel<<<g, cl::NT, 0, st>>>(order, w->r, n, nv, dr_tol, w->flag);
             e = cudaGetLastError();
         }
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(w->h_counters + 1, w->counters + 1, sizeof(unsigned),
-                                cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) goto fail;
+        if (e == cudaSuccess) {
+            tb = w->temp_bytes;
+            e = cub::DeviceScan::ExclusiveSum(w->temp, tb, w->flag, w->runid, (int)n, st);
+        }
+        if (e == cudaSuccess) {
+            cl::run_pick_kernel<<<g, cl::NT, 0, st>>>(order, w->metric, w->flag, w->runid, nv,
+                                                      w->list);
+            cl::count_runs_kernel<<<1, 1, 0, st>>>(w->flag, w->runid, n, m);
+            e = cudaGetLastError();
+        }
         listp = w->list;
-        mlen = w->h_counters[1];
     } else {
+        if (e == cudaSuccess) {
+            cl::copy_count_kernel<<<1, 1, 0, st>>>(nv, m);
+            e = cudaGetLastError();
+        }
         listp = order;
-        mlen = nv;
     }
-    if (harm_remove && mlen > 0) {
-        const unsigned gm = (mlen + cl::NT - 1) / cl::NT;
-        cl::gather_metric_kernel<<<gm, cl::NT, 0, st>>>(listp, w->metric, mlen, w->mkey[0],
-                                                        w->mpos[0]);
-        e = cudaGetLastError();
+    if (harm_remove) {
+        if (e == cudaSuccess) {
+            cl::gather_metric_kernel<<<g, cl::NT, 0, st>>>(listp, w->metric, n, m, w->mkey[0],
+                                                           w->mpos[0]);
+            e = cudaGetLastError();
+        }
         cub::DoubleBuffer<double> mb(w->mkey[0], w->mkey[1]);
         cub::DoubleBuffer<unsigned> pb(w->mpos[0], w->mpos[1]);
         if (e == cudaSuccess) {
             tb = w->temp_bytes;
-            e = cub::DeviceRadixSort::SortPairsDescending(w->temp, tb, mb, pb, (int)mlen, 0, 64,
-                                                          st);
+            e = cub::DeviceRadixSort::SortPairsDescending(w->temp, tb, mb, pb, (int)n, 0, 64, st);
         }
         if (e == cudaSuccess) {
-            cl::greedy_kernel<<<1, 1024, 0, st>>>(listp, pb.Current(), w->r, mlen, numharm,
+            cl::greedy_kernel<<<1, 1024, 0, st>>>(listp, pb.Current(), w->r, m, numharm,
                                                   harm_tol, w->removed, w->keep);
             e = cudaGetLastError();
         }
         keep = w->keep;
     }
     if (e == cudaSuccess) {
-        cl::emit_kernel<<<1, 1024, 0, st>>>(listp, keep, mlen, w->r, w->freq, w->metric,
-                                            w->nharm, w->out, w->counters + 2);
+        cl::emit_kernel<<<1, 1024, 0, st>>>(listp, keep, m, w->r, w->freq, w->metric,
+                                            w->nharm, w->out, nout);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(w->h_counters + 2, w->counters + 2, sizeof(unsigned),
+        e = cudaMemcpyAsync(w->h_counters, w->counters, 4 * sizeof(unsigned),
                             cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "Error: candidate collapse on the GPU: %s\n", cudaGetErrorString(e));
+        return -1;
+    }
+    return 0;
+}
+
+int cs_collapse_finish(CsCollapse *w, cudaStream_t st, CandidateList *out)
+{
+    candlist_init(out);
+    if (!w) return -1;
+    if (w->pending_n == 0) return 0;
+    cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) goto fail;
-    nout = w->h_counters[2];
-    if (nout > w->h_out_cap) {
-        if (w->h_out) cudaFreeHost(w->h_out);
-        w->h_out = nullptr;
-        w->h_out_cap = 0;
-        e = cudaMallocHost((void **)&w->h_out, (size_t)(nout + nout / 4 + 256) * sizeof(Candidate));
-        if (e != cudaSuccess) goto fail;
-        w->h_out_cap = nout + nout / 4 + 256;
+    {
+        const unsigned nout = w->h_counters[2];
+        if (nout > w->h_out_cap) {
+            if (w->h_out) cudaFreeHost(w->h_out);
+            w->h_out = nullptr;
+            w->h_out_cap = 0;
+            e = cudaMallocHost((void **)&w->h_out,
+                               (size_t)(nout + nout / 4 + 256) * sizeof(Candidate));
+            if (e != cudaSuccess) goto fail;
+            w->h_out_cap = nout + nout / 4 + 256;
+        }
+        if (nout) {
+            e = cudaMemcpyAsync(w->h_out, w->out, (size_t)nout * sizeof(Candidate),
+                                cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) goto fail;
+            out->v = (Candidate *)malloc((size_t)nout * sizeof(Candidate));
+            if (!out->v) return -1;
+            memcpy(out->v, w->h_out, (size_t)nout * sizeof(Candidate));
+            out->n = nout;
+            out->cap = nout;
+        }
     }
-    if (nout) {
-        e = cudaMemcpyAsync(w->h_out, w->out, (size_t)nout * sizeof(Candidate),
-                            cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) goto fail;
-        out->v = (Candidate *)malloc((size_t)nout * sizeof(Candidate));
-        if (!out->v) return -1;
-        memcpy(out->v, w->h_out, (size_t)nout * sizeof(Candidate));
-        out->n = nout;
-        out->cap = nout;
-    }
+    w->pending_n = 0;
     return 0;
 fail:
     fprintf(stderr, "Error: candidate collapse on the GPU: %s\n", cudaGetErrorString(e));

@@ -1284,13 +1284,11 @@ CS_EXPORT int cs_b200_session_collect(GpuSession *S, double threshold, Candidate
     return rerun ? 1 : 0;
 }
 
-CS_EXPORT int cs_b200_session_collect_collapsed(GpuSession *S, double threshold, int remove,
-                                                double dr_tol, int harm_remove, int numharm,
-                                                double harm_tol, CandidateList *out,
-                                                float *kernel_ms)
+CS_EXPORT int cs_b200_session_collapse_enqueue(GpuSession *S, double threshold, int remove,
+                                               double dr_tol, int harm_remove, int numharm,
+                                               double harm_tol)
 {
-    if (!S || !out) return -1;
-    candlist_init(out);
+    if (!S) return -1;
     cudaError_t e;
     if ((e = cudaMemcpyAsync(S->h_count, S->d_count, sizeof(unsigned), cudaMemcpyDeviceToHost,
                              S->st)) != cudaSuccess ||
@@ -1304,11 +1302,6 @@ CS_EXPORT int cs_b200_session_collect_collapsed(GpuSession *S, double threshold,
         fprintf(stderr, "Error: B200 search kernel timed out waiting for the tensor cores\n");
         return -1;
     }
-    if (kernel_ms) {
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, S->ev0, S->ev1);
-        *kernel_ms = ms;
-    }
     const unsigned n = S->h_count[0];
     if (n > S->cap) {
         if (grow_records(S, n + n / 8 + 1024) != 0) return -1;
@@ -1320,10 +1313,36 @@ CS_EXPORT int cs_b200_session_collect_collapsed(GpuSession *S, double threshold,
         k[i] = S->tab.slot[i].k;
         Hk[i] = S->tab.slot[i].Hk;
     }
-    return cs_collapse_run(S->coll, S->d_recs, n, S->d_chunks, S->tab.nchunks, k, Hk,
-                           S->tab.nslot, S->Nprof, S->r_lo, S->lodr, (double)S->N, S->T,
-                           threshold, remove, dr_tol, harm_remove, numharm, harm_tol, S->st,
-                           out) == 0 ? 0 : -1;
+    return cs_collapse_enqueue(S->coll, S->d_recs, n, S->d_chunks, S->tab.nchunks, k, Hk,
+                               S->tab.nslot, S->Nprof, S->r_lo, S->lodr, (double)S->N, S->T,
+                               threshold, remove, dr_tol, harm_remove, numharm, harm_tol,
+                               S->st) == 0 ? 0 : -1;
+}
+
+CS_EXPORT int cs_b200_session_collapse_wait(GpuSession *S, CandidateList *out, float *kernel_ms)
+{
+    if (!S || !out) return -1;
+    candlist_init(out);
+    if (kernel_ms) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, S->ev0, S->ev1);
+        *kernel_ms = ms;
+    }
+    if (!S->coll) return 0;
+    return cs_collapse_finish(S->coll, S->st, out) == 0 ? 0 : -1;
+}
+
+CS_EXPORT int cs_b200_session_collect_collapsed(GpuSession *S, double threshold, int remove,
+                                                double dr_tol, int harm_remove, int numharm,
+                                                double harm_tol, CandidateList *out,
+                                                float *kernel_ms)
+{
+    if (!S || !out) return -1;
+    candlist_init(out);
+    const int rc = cs_b200_session_collapse_enqueue(S, threshold, remove, dr_tol, harm_remove,
+                                                    numharm, harm_tol);
+    if (rc != 0) return rc;
+    return cs_b200_session_collapse_wait(S, out, kernel_ms);
 }
 
 CS_EXPORT float *cs_b200_session_device_amps(GpuSession *S)

@@ -152,6 +152,11 @@ def declare_gpu_api(lib: C.CDLL) -> C.CDLL:
                                                       C.c_double, C.c_int, C.c_int, C.c_double,
                                                       P(CandidateList), P(C.c_float)]
     lib.cs_b200_session_collect_collapsed.restype = C.c_int
+    lib.cs_b200_session_collapse_enqueue.argtypes = [C.c_void_p, C.c_double, C.c_int,
+                                                     C.c_double, C.c_int, C.c_int, C.c_double]
+    lib.cs_b200_session_collapse_enqueue.restype = C.c_int
+    lib.cs_b200_session_collapse_wait.argtypes = [C.c_void_p, P(CandidateList), P(C.c_float)]
+    lib.cs_b200_session_collapse_wait.restype = C.c_int
     lib.cs_b200_session_sync.argtypes = [C.c_void_p]
     lib.cs_b200_session_sync.restype = C.c_int
     lib.cs_b200_session_search_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_double,

@@ -30,9 +30,11 @@ def running_mean(x: np.ndarray) -> float:
 class PrepSearch:
     """Dedisperse a filterbank and search every DM series on one GPU.
 
-    Two search sessions of the one geometry alternate over the DMs: while DM
-    d is searched on one, DM d+1's spectrum is made on the prep stream into
-    the other's spectrum buffer and DM d-1's candidates are read back."""
+    Three search sessions of the one geometry take the DMs in turn.  At DM i
+    the host queues DM i's spectrum (prep stream) and search, then DM i-1's
+    collapse, then waits for DM i-2's list, so the GPU always has the next
+    search queued behind the collapse work.  Without collapsing, DM i-1's raw
+    records are read back while DM i is searched."""
 
     def __init__(self, tables: DedispTables, nspec: int, numout: int, dt: float,
                  opts: Options | None = None, device: int = 0):
@@ -52,7 +54,7 @@ class PrepSearch:
         self.out = torch.empty((tables.ndm, self.stride), dtype=torch.float32, device=self.dev)
         self.stream = torch.cuda.Stream(device=self.dev)
         self.spec = SpectrumMaker(self.N, dt, device=device)
-        self.sessions = [Session(self.N, dt, self.opts, device=device) for _ in range(2)]
+        self.sessions = [Session(self.N, dt, self.opts, device=device) for _ in range(3)]
         self.ses = self.sessions[0]
         self.pad_value = None
         self.search_ms: list[float] = []     # search kernel time of each DM, last pass
@@ -78,39 +80,61 @@ class PrepSearch:
         self.spec.run_device(self.out[d].data_ptr(), ses.device_amps_ptr(),
                              self.stream.cuda_stream)
 
-    def _finish(self, ses: Session, threshold: float | None, collapse: bool = False) -> np.ndarray:
-        get = ses.collect_collapsed if collapse else ses.collect
-        out, ms, rc = get(threshold)
-        if rc == 1:                     # record buffer grown: run again
-            ses.enqueue(None, threshold)
-            out, ms, rc = get(threshold)
-        self.search_ms.append(ms)
-        return out
-
     def search_dm(self, d: int, threshold: float | None = None) -> np.ndarray:
         """Spectrum and search of DM d's series: raw candidates."""
         ses = self.sessions[0]
         self._spectrum(d, ses)
         ses.enqueue(None, threshold, after_stream=self.stream.cuda_stream)
-        return self._finish(ses, threshold)
+        out, _, rc = ses.collect(threshold)
+        if rc == 1:                     # record buffer grown: run again
+            ses.enqueue(None, threshold)
+            out, _, rc = ses.collect(threshold)
+        return out
 
     def search_all(self, threshold: float | None = None, dms=None,
                    collapse: bool = False) -> list[np.ndarray]:
-        """Candidates of every DM (or of `dms`), pipelined over the two
-        sessions, in DM order: raw, or with `collapse` the list search_file
-        returns, collapsed on the GPU."""
+        """Candidates of every DM (or of `dms`) in DM order: raw, or with
+        `collapse` the list search_file returns, collapsed on the GPU."""
         dms = list(range(self.t.ndm)) if dms is None else list(dms)
-        res: list[np.ndarray] = []
-        self.search_ms = []
+        self.search_ms = [0.0] * len(dms)
+        S, ns = self.sessions, len(self.sessions)
+        res: list = [None] * len(dms)
+
+        def start_collapse(j: int) -> None:
+            ses = S[j % ns]
+            while ses.collapse_enqueue(threshold) == 1:   # record buffer grown
+                ses.enqueue(None, threshold)
+
+        def finish(j: int) -> None:
+            if collapse:
+                res[j], self.search_ms[j] = S[j % ns].collapse_wait()
+            else:
+                ses = S[j % ns]
+                out, ms, rc = ses.collect(threshold)
+                if rc == 1:
+                    ses.enqueue(None, threshold)
+                    out, ms, rc = ses.collect(threshold)
+                res[j], self.search_ms[j] = out, ms
+
         for i, d in enumerate(dms):
-            ses = self.sessions[i & 1]
-            # ses's previous search (DM i-2) was collected in iteration i-1
+            ses = S[i % ns]          # its last DM, i - ns, was finished at i - 1
             self._spectrum(d, ses)
             ses.enqueue(None, threshold, after_stream=self.stream.cuda_stream)
-            if i > 0:
-                res.append(self._finish(self.sessions[(i - 1) & 1], threshold, collapse))
-        if dms:
-            res.append(self._finish(self.sessions[(len(dms) - 1) & 1], threshold, collapse))
+            if collapse:
+                if i >= 1:
+                    start_collapse(i - 1)
+                if i >= 2:
+                    finish(i - 2)
+            elif i >= 1:
+                finish(i - 1)
+        n = len(dms)
+        if collapse:
+            if n >= 1:
+                start_collapse(n - 1)
+            for j in range(max(0, n - 2), n):
+                finish(j)
+        elif n >= 1:
+            finish(n - 1)
         return res
 
     def run(self, d_raw: int, nspec: int, collapse: bool = True) -> list[np.ndarray]:

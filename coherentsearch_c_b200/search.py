@@ -205,6 +205,28 @@ class Session:
         self.host.candlist_free(C.byref(cl))
         return out, ms.value, rc
 
+    def collapse_enqueue(self, threshold: float | None = None) -> int:
+        """First half of collect_collapsed: waits for the search, queues the
+        collapse; returns 0, or 1 when the record buffer was grown (enqueue
+        the search again)."""
+        thr = self.opts.threshold if threshold is None else threshold
+        o = self.opts
+        rc = self.gpu.cs_b200_session_collapse_enqueue(self.sess, thr, int(o.remove), o.drtol,
+                                                       int(o.harm_remove), o.numharm, 1.0)
+        if rc < 0:
+            raise RuntimeError("collapse_enqueue failed")
+        return rc
+
+    def collapse_wait(self):
+        """Second half: (candidates, kernel ms)."""
+        cl = nt.CandidateList()
+        ms = C.c_float(0)
+        if self.gpu.cs_b200_session_collapse_wait(self.sess, C.byref(cl), C.byref(ms)) != 0:
+            raise RuntimeError("collapse_wait failed")
+        out = nt.candidates_to_numpy(cl)
+        self.host.candlist_free(C.byref(cl))
+        return out, ms.value
+
     def measure_ducy(self, cands: np.ndarray) -> np.ndarray:
         """measure_ducy (src/candidate.c:305-329) on the GPU against the
         spectrum this session last searched (still in device memory): a copy

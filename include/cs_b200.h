@@ -63,6 +63,16 @@ int cs_b200_session_collect_collapsed(GpuSession *s, double threshold, int remov
                                       double dr_tol, int harm_remove, int numharm,
                                       double harm_tol, CandidateList *out, float *kernel_ms);
 
+/* The two halves of cs_b200_session_collect_collapsed.  _enqueue waits for
+ * the search (it reads the record count), then queues the collapse on the
+ * session stream and returns 0, 1 (record buffer grown: enqueue the search
+ * again) or -1; _wait synchronises and hands over the list.  Between the
+ * two the caller can queue work for other sessions. */
+int cs_b200_session_collapse_enqueue(GpuSession *s, double threshold, int remove,
+                                     double dr_tol, int harm_remove, int numharm,
+                                     double harm_tol);
+int cs_b200_session_collapse_wait(GpuSession *s, CandidateList *out, float *kernel_ms);
+
 /* ---- batched search of many spectra -------------------------------------
  * No reference counterpart: the reference searches one file per call
  * (src/search.c:1388-1406) and rebuilds its GPU session whenever the file
