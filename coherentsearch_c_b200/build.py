@@ -34,10 +34,11 @@ HOST_COMMON = ["cs_common.c"]
 HOST_GPU_ONLY = ["cs_tables.c"]
 HOST_LIB = ["cs_common.c", "cs_search.c"]
 CUDA_SRCS = ["cs_gpu.cu", "cs_dedisp.cu", "cs_spectrum.cu", "cs_ducy.cu",
-             "cs_collapse.cu"]
+             "cs_collapse.cu", "cs_clip.cu"]
 # FP64 candidate arithmetic that must round like the host restatements, which
 # are built with -ffp-contract=off: no multiply-add contraction
-CUDA_FLAGS = {"cs_ducy.cu": ["-fmad=false"], "cs_collapse.cu": ["-fmad=false"]}
+CUDA_FLAGS = {"cs_ducy.cu": ["-fmad=false"], "cs_collapse.cu": ["-fmad=false"],
+              "cs_clip.cu": ["-fmad=false"]}
 
 
 def _run(cmd, verbose):

@@ -1,0 +1,236 @@
+/*
+ * The decisions of prepsubband's time-domain clipping on the GPU: which
+ * spectra PRESTO's clip_times (third_party/presto/src/clipping.c:47-230)
+ * replaces when the reference runs its front end with -clip clip_sigma (its
+ * default is 6).  clip_times runs on every raw block of L spectra in read
+ * order (backend_common.c:976-986), with running statistics carried from
+ * block to block:
+ *
+ *   zero-DM series   the sum of each spectrum over all channels (exact for
+ *                    8-bit data: an integer below 2^24 as a float);
+ *   block stats      avg_var (misc_utils.c:641-676, AS 52 recurrence in
+ *                    double) and the lower median (median.c, element
+ *                    (L-1)/2 of the sorted block); the "good" samples lie
+ *                    strictly inside median -+ 3 sigma (float cut-offs), and
+ *                    their avg_var gives the block's mean and sigma (the
+ *                    running values stand in when no sample is good);
+ *   running values   floats: mean and sigma of the first block, then
+ *                    0.9 * old + 0.1 * new, evaluated in double;
+ *   decision         spectrum t is replaced when
+ *                    |zdm[t] - running_mean| > clip_sigma * running_sigma
+ *                    (the difference in float, the test in double).
+ *
+ * The replacement values (channel running levels) are not produced: the
+ * device front end implements prepsubband without clipping, and a run with
+ * -clip is the same run exactly when this count is zero.  The arithmetic is
+ * the reference's without fast-math rewriting (this file is built with
+ * -fmad=false); the reference's -Ofast build can move its sigma in the last
+ * bits, which only matters for a spectrum within that distance of the
+ * trigger.
+ */
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+
+#include "cs_b200.h"
+
+#define CS_EXPORT extern "C" __attribute__((visibility("default")))
+
+namespace ck {
+
+constexpr int MAX_L = 8192;
+constexpr int NT = 256;
+
+/* zero-DM sum of each spectrum: one warp per spectrum */
+__global__ void zdm_kernel(const uint8_t *raw, long long nspec, int nchan, int vec16, int *zdm)
+{
+    const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (t >= nspec) return;
+    const uint8_t *row = raw + t * (long long)nchan;
+    unsigned s = 0;
+    if (vec16) {
+        const uint4 *r4 = reinterpret_cast<const uint4 *>(row);
+        for (int i = lane; i < nchan / 16; i += 32) {
+            const uint4 w = __ldg(r4 + i);
+            s = __dp4a(w.x, 0x01010101u, s);
+            s = __dp4a(w.y, 0x01010101u, s);
+            s = __dp4a(w.z, 0x01010101u, s);
+            s = __dp4a(w.w, 0x01010101u, s);
+        }
+    } else {
+        for (int c = lane; c < nchan; c += 32) s += row[c];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) zdm[t] = (int)s;
+}
+
+/* avg_var (misc_utils.c:641-676) over n floats, in order */
+struct AvgVar {
+    double mean = 0.0, var_acc = 0.0, an1 = 0.0;
+    long n = 0;
+    __device__ void push(float x)
+    {
+        if (n == 0) {
+            mean = (double)x;
+        } else {
+            const double an = (double)(n + 1);
+            an1 = (double)n;
+            const double dx = ((double)x - mean) / an;
+            var_acc += an * an1 * dx * dx;
+            mean += dx;
+        }
+        n++;
+    }
+    __device__ double var() const { return n > 1 ? var_acc / an1 : var_acc; }
+};
+
+struct BlockStats {
+    int ngood;
+    double mean, sigma;      /* of the good samples */
+};
+
+/* one CTA per block: lower median by a shared-memory sort, then the two
+ * sequential avg_var passes on one thread */
+__global__ void __launch_bounds__(NT) block_kernel(const int *zdm, int L, int P2,
+                                                   BlockStats *out)
+{
+    extern __shared__ int sm[];
+    int *x = sm, *srt = sm + L;
+    const long long b = blockIdx.x;
+    for (int i = threadIdx.x; i < P2; i += NT) {
+        const int v = i < L ? zdm[b * L + i] : INT_MAX;
+        if (i < L) x[i] = v;
+        srt[i] = v;
+    }
+    __syncthreads();
+    for (int k = 2; k <= P2; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < P2; i += NT) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const bool up = (i & k) == 0;
+                    const int a = srt[i], c = srt[l];
+                    if ((a > c) == up) { srt[i] = c; srt[l] = a; }
+                }
+            }
+            __syncthreads();
+        }
+    if (threadIdx.x != 0) return;
+    AvgVar all;
+    for (int i = 0; i < L; i++) all.push((float)x[i]);
+    const double sd = sqrt(all.var());
+    const float med = (float)srt[(L - 1) / 2];
+    const float lo = (float)((double)med - 3.0 * sd);
+    const float hi = (float)((double)med + 3.0 * sd);
+    AvgVar good;
+    for (int i = 0; i < L; i++) {
+        const float v = (float)x[i];
+        if (v > lo && v < hi) good.push(v);
+    }
+    BlockStats s;
+    s.ngood = (int)good.n;
+    s.mean = good.mean;
+    s.sigma = good.n ? sqrt(good.var()) : 0.0;
+    out[b] = s;
+}
+
+/* the running mean / sigma from block to block (one thread) */
+__global__ void running_kernel(const BlockStats *st, long long nblocks, float clip_sigma,
+                               float *ravg, float *trig)
+{
+    float running_avg = 0.0f, running_std = 0.0f;
+    for (long long b = 0; b < nblocks; b++) {
+        double cur_avg, cur_std;
+        if (st[b].ngood < 1) {
+            cur_avg = (double)running_avg;
+            cur_std = (double)running_std;
+        } else {
+            cur_avg = st[b].mean;
+            cur_std = st[b].sigma;
+        }
+        if (b) {
+            running_avg = (float)(0.9 * (double)running_avg + 0.1 * cur_avg);
+            running_std = (float)(0.9 * (double)running_std + 0.1 * cur_std);
+        } else {
+            running_avg = (float)cur_avg;
+            running_std = (float)cur_std;
+        }
+        ravg[b] = running_avg;
+        trig[b] = clip_sigma * running_std;
+    }
+}
+
+__global__ void decide_kernel(const int *zdm, long long n, int L, const float *ravg,
+                              const float *trig, unsigned long long *count, uint8_t *flags)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const long long b = t / L;
+    const float d = (float)zdm[t] - ravg[b];
+    const bool clip = fabs((double)d) > (double)trig[b];
+    if (flags) flags[t] = clip ? 1 : 0;
+    if (clip) atomicAdd(count, 1ull);
+}
+
+}  // namespace ck
+
+CS_EXPORT int cs_clip_count(const uint8_t *d_raw, long long nspec, int nchan, int L,
+                            float clip_sigma, long long *nclipped, uint8_t *d_flags,
+                            void *stream, int device)
+{
+    if (!nclipped || nchan < 1 || L < 1 || L > ck::MAX_L || nspec < 0) return -1;
+    *nclipped = 0;
+    const long long nblocks = nspec / L;     /* a partial last block is never read */
+    if (nblocks == 0 || !(clip_sigma > 0.0f)) return 0;
+    if (!d_raw) return -1;
+    if (cudaSetDevice(device) != cudaSuccess) return -1;
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long n = nblocks * L;
+    int P2 = 1;
+    while (P2 < L) P2 <<= 1;
+    const size_t smem = (size_t)(L + P2) * sizeof(int);
+    int *zdm = nullptr;
+    ck::BlockStats *bs = nullptr;
+    float *ravg = nullptr, *trig = nullptr;
+    unsigned long long *cnt = nullptr, hcnt = 0;
+    cudaError_t e = cudaMalloc((void **)&zdm, (size_t)n * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&bs, (size_t)nblocks * sizeof(ck::BlockStats));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&ravg, (size_t)nblocks * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&trig, (size_t)nblocks * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&cnt, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st);
+    if (e == cudaSuccess && smem > 48 * 1024)
+        e = cudaFuncSetAttribute((const void *)ck::block_kernel,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) {
+        const int vec16 = (nchan % 16 == 0) && (((uintptr_t)d_raw & 15) == 0);
+        const long long threads = n * 32;
+        ck::zdm_kernel<<<(unsigned)((threads + ck::NT - 1) / ck::NT), ck::NT, 0, st>>>(
+            d_raw, n, nchan, vec16, zdm);
+        ck::block_kernel<<<(unsigned)nblocks, ck::NT, smem, st>>>(zdm, L, P2, bs);
+        ck::running_kernel<<<1, 1, 0, st>>>(bs, nblocks, clip_sigma, ravg, trig);
+        ck::decide_kernel<<<(unsigned)((n + ck::NT - 1) / ck::NT), ck::NT, 0, st>>>(
+            zdm, n, L, ravg, trig, cnt, d_flags);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&hcnt, cnt, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(zdm);
+    cudaFree(bs);
+    cudaFree(ravg);
+    cudaFree(trig);
+    cudaFree(cnt);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "Error: cs_clip_count: %s\n", cudaGetErrorString(e));
+        return -1;
+    }
+    *nclipped = (long long)hcnt;
+    return 0;
+}

@@ -65,6 +65,7 @@ class Dedisperser:
 
     def __init__(self, tables: DedispTables, max_spectra: int, device: int = 0):
         self.t = tables
+        self.device = device
         self.lib = nt.gpu_lib()
         ip = C.POINTER(C.c_int)
         self._idisp = np.ascontiguousarray(tables.idispdt, np.int32)
@@ -103,6 +104,18 @@ class Dedisperser:
         if rc != 0:
             raise RuntimeError("cs_dedisp_run_device failed (see stderr)")
         return got.value
+
+    def clip_count(self, d_raw: int, nspec: int, clip_sigma: float = 6.0,
+                   stream: int | None = None) -> int:
+        """cs_clip_count: the spectra prepsubband's -clip clip_sigma would
+        replace in this filterbank (0: the unclipped output is the clipped
+        run's)."""
+        n = C.c_longlong(0)
+        rc = self.lib.cs_clip_count(d_raw, nspec, self.t.nchan, self.t.spectra_per_subint,
+                                    float(clip_sigma), C.byref(n), None, stream, self.device)
+        if rc != 0:
+            raise RuntimeError("cs_clip_count failed (see stderr)")
+        return n.value
 
     def last_times(self) -> tuple[float, float]:
         a, b = C.c_float(0), C.c_float(0)

@@ -37,7 +37,7 @@ class PrepSearch:
     records are read back while DM i is searched."""
 
     def __init__(self, tables: DedispTables, nspec: int, numout: int, dt: float,
-                 opts: Options | None = None, device: int = 0):
+                 opts: Options | None = None, device: int = 0, clip_sigma: float = 6.0):
         import torch
         self.torch = torch
         self.t = tables
@@ -57,6 +57,9 @@ class PrepSearch:
         self.sessions = [Session(self.N, dt, self.opts, device=device) for _ in range(3)]
         self.ses = self.sessions[0]
         self.pad_value = None
+        # prepsubband clips at 6 sigma unless told -noclip (0 here): the device
+        # path has no clipping, so it checks that clipping would change nothing
+        self.clip_sigma = float(clip_sigma)
         self.search_ms: list[float] = []     # search kernel time of each DM, last pass
 
     def dedisperse(self, d_raw: int, nspec: int) -> None:
@@ -65,6 +68,13 @@ class PrepSearch:
         torch = self.torch
         # the raw block may still be in flight on the caller's stream
         self.stream.wait_stream(torch.cuda.current_stream(self.dev))
+        if self.clip_sigma > 0:
+            n = self.dd.clip_count(d_raw, nspec, self.clip_sigma, self.stream.cuda_stream)
+            if n:
+                raise RuntimeError(
+                    f"prepsubband's -clip {self.clip_sigma:g} would replace {n} spectra of this "
+                    "filterbank; the device front end has no clipping (pass clip_sigma=0 for "
+                    "the unclipped series, prepsubband's -noclip)")
         n = self.dd.run_device(d_raw, nspec, self.out.data_ptr(), self.stride, self.N,
                                self.stream.cuda_stream)
         if n != self.nout:

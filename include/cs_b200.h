@@ -145,6 +145,19 @@ int cs_ducy_run_device(CsDucy *d, const float *d_amps, long long namps, long lon
                        void *stream);
 void cs_ducy_free(CsDucy *d);
 
+/* ---- prepsubband's time-domain clipping: decisions only ---------------
+ * How many spectra PRESTO's clip_times (third_party/presto/src/clipping.c)
+ * would replace when the reference's front end runs with -clip clip_sigma
+ * (its default, 6) on the 8-bit filterbank at d_raw ([nspec][nchan], SIGPROC
+ * order): every full block of L spectra, running statistics carried from
+ * block to block.  d_flags (device, nspec / L * L bytes, may be NULL) gets 1
+ * for each such spectrum.  The device front end runs without clipping; its
+ * output equals the clipped run's exactly when *nclipped is 0 (counted over
+ * every full block, also ones a run with a shorter numout never reads).
+ * Returns 0 or -1. */
+int cs_clip_count(const uint8_t *d_raw, long long nspec, int nchan, int L, float clip_sigma,
+                  long long *nclipped, uint8_t *d_flags, void *stream, int device);
+
 /* The value prepsubband pads every DM series with: PRESTO's running mean
  * (update_stats) of DM 0's n output samples.  In libcoherent_search.so. */
 double cs_prep_pad_value(const float *x, long long n);

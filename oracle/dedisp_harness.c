@@ -23,6 +23,13 @@
  *                    numout points)
  *
  * Compiled with -Ofast like the reference's PREP sources (src/Makefile:152-161).
+ *
+ * odd_run_clip adds PRESTO's time-domain clipping (clipping.c clip_times,
+ * with median.c and misc_utils.c's avg_var, compiled into the same library)
+ * at its place in prep_subbands (backend_common.c:976-986): on each raw block
+ * in time-major PRESTO channel order, before the transpose.  clip_times keeps
+ * its running averages in static variables, so a clipped run needs a fresh
+ * copy of this library.
  */
 #include <math.h>
 #include <stdlib.h>
@@ -38,6 +45,23 @@ void dedisp_subbands(float *data, float *lastdata, int numpts, int numchan, int 
 void float_dedisp(float *data, float *lastdata, int numpts, int numchan, int *delays,
                   float approx_mean, float *result, int transpose);
 void vect_free(void *vect);
+int clip_times(float *rawdata, int ptsperblk, int numchan, float clip_sigma,
+               float *good_chan_levels, int thread);
+
+/* Two functions the linked PRESTO files reference outside the clipping path:
+ * misc_utils.c's date helpers call SLALIB's slaDjcl, and clip_times opens a
+ * bin file only when CLIPBINSFILE is set (neither is reached here). */
+#include <stdio.h>
+void slaDjcl(double djm, int *iy, int *im, int *id, double *fd, int *j)
+{
+    (void)djm; *iy = *im = *id = 0; *fd = 0.0; *j = 1;
+}
+FILE *chkfopen(char *path, const char *mode)
+{
+    FILE *f = fopen(path, mode);
+    if (!f) { perror(path); exit(1); }
+    return f;
+}
 
 #define NEAREST_LONG(x) (long) (x < 0 ? ceil(x - 0.5) : floor(x + 0.5))
 
@@ -94,15 +118,31 @@ typedef struct {
     long long next;          /* next block to read */
 } Reader;
 
-/* One block converted to PRESTO order and transposed channel-major;
- * 0 when no full block is left. */
+/* One block converted to PRESTO order, clipped when clip_sigma > 0, and
+ * transposed channel-major; 0 when no full block is left. */
+static float g_clip_sigma;
+static float *g_timemajor, *g_padvals;
+static long long g_nclipped;
+
 static int read_block(Reader *r, float *chanmajor)
 {
     if ((r->next + 1) * (long long)r->L > r->nspec) return 0;
     const unsigned char *b = r->raw + r->next * (long long)r->L * r->nchan;
-    for (int t = 0; t < r->L; t++)
-        for (int c = 0; c < r->nchan; c++)
-            chanmajor[(long long)c * r->L + t] = (float)b[(long long)t * r->nchan + (r->nchan - 1 - c)];
+    if (g_clip_sigma > 0.0f) {
+        for (int t = 0; t < r->L; t++)
+            for (int c = 0; c < r->nchan; c++)
+                g_timemajor[(long long)t * r->nchan + c] =
+                    (float)b[(long long)t * r->nchan + (r->nchan - 1 - c)];
+        g_nclipped += clip_times(g_timemajor, r->L, r->nchan, g_clip_sigma, g_padvals, 1);
+        for (int t = 0; t < r->L; t++)
+            for (int c = 0; c < r->nchan; c++)
+                chanmajor[(long long)c * r->L + t] = g_timemajor[(long long)t * r->nchan + c];
+    } else {
+        for (int t = 0; t < r->L; t++)
+            for (int c = 0; c < r->nchan; c++)
+                chanmajor[(long long)c * r->L + t] =
+                    (float)b[(long long)t * r->nchan + (r->nchan - 1 - c)];
+    }
     r->next++;
     return 1;
 }
@@ -170,4 +210,23 @@ int odd_run(const unsigned char *raw, long long nspec, int nchan, int nsub, int 
     *nout_written = totwrote;
     free(raw1); free(raw2); free(cur); free(last); free(tmp); free(idisp); free(offs);
     return 0;
+}
+
+/* odd_run with prepsubband's -clip clip_sigma; *nclipped = spectra replaced. */
+int odd_run_clip(const unsigned char *raw, long long nspec, int nchan, int nsub, int ndm,
+                 int L, int bpr, const int *idispdt, const int *offsets_in, long long numout,
+                 float *out, long long out_stride, long long *nout_written, float clip_sigma,
+                 long long *nclipped)
+{
+    g_clip_sigma = clip_sigma;
+    g_nclipped = 0;
+    g_timemajor = calloc((size_t)L * nchan, sizeof(float));
+    g_padvals = calloc((size_t)nchan, sizeof(float));
+    const int rc = odd_run(raw, nspec, nchan, nsub, ndm, L, bpr, idispdt, offsets_in, numout,
+                           out, out_stride, nout_written);
+    free(g_timemajor); free(g_padvals);
+    g_timemajor = g_padvals = NULL;
+    g_clip_sigma = 0.0f;
+    *nclipped = g_nclipped;
+    return rc;
 }

@@ -298,18 +298,46 @@ def ref_dedisp_tables(nchan, nsub, ndm, lodm, dmstep, lofreq, chanwid, dt, L=240
     return idisp, offs, bpr.value, avg.value
 
 
-def ref_dedisp_run(raw, nsub, idisp, offs, L, bpr, numout=-1):
-    """The reference's prepsubband output for every DM: [ndm][nout] float32."""
-    lib = dedisp_ref_lib()
+def _fresh_dedisp_lib() -> C.CDLL:
+    """A private copy of libdedisp_ref.so: clip_times keeps its running
+    averages in static variables (clipping.c:55-59), so every clipped run
+    starts from a new instance, as a prepsubband process does."""
+    import shutil
+    import tempfile
+    d = tempfile.mkdtemp(prefix="ddref")
+    path = os.path.join(d, "libdedisp_ref.so")
+    shutil.copy(os.path.join(REF_DIR, "libdedisp_ref.so"), path)
+    lib = C.CDLL(path)
+    IP = C.POINTER(C.c_int)
+    lib.odd_run_clip.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_int, C.c_int,
+                                 C.c_int, IP, IP, C.c_longlong, C.c_void_p, C.c_longlong,
+                                 C.POINTER(C.c_longlong), C.c_float, C.POINTER(C.c_longlong)]
+    return lib
+
+
+def ref_dedisp_run(raw, nsub, idisp, offs, L, bpr, numout=-1, clip_sigma=0.0,
+                   return_clipped=False):
+    """The reference's prepsubband output for every DM: [ndm][nout] float32.
+    With clip_sigma > 0, PRESTO's clip_times runs on each raw block as
+    prepsubband's -clip does; return_clipped adds the number of spectra it
+    replaced."""
+    lib = dedisp_ref_lib() if clip_sigma <= 0 else _fresh_dedisp_lib()
     raw = np.ascontiguousarray(raw, np.uint8)
     nspec, nchan = raw.shape
     ndm = offs.shape[0]
     cap = nspec if numout < 0 else min(numout, nspec)
     out = np.zeros((ndm, max(cap, 1)), np.float32)
     got = C.c_longlong(0)
+    nclip = C.c_longlong(0)
     IP = C.POINTER(C.c_int)
     idisp = np.ascontiguousarray(idisp, np.int32)
     offs = np.ascontiguousarray(offs, np.int32)
-    lib.odd_run(raw.ctypes.data, nspec, nchan, nsub, ndm, L, bpr, idisp.ctypes.data_as(IP),
-                offs.ctypes.data_as(IP), cap, out.ctypes.data, out.shape[1], C.byref(got))
-    return out[:, :got.value]
+    if clip_sigma > 0:
+        lib.odd_run_clip(raw.ctypes.data, nspec, nchan, nsub, ndm, L, bpr,
+                         idisp.ctypes.data_as(IP), offs.ctypes.data_as(IP), cap, out.ctypes.data,
+                         out.shape[1], C.byref(got), float(clip_sigma), C.byref(nclip))
+    else:
+        lib.odd_run(raw.ctypes.data, nspec, nchan, nsub, ndm, L, bpr, idisp.ctypes.data_as(IP),
+                    offs.ctypes.data_as(IP), cap, out.ctypes.data, out.shape[1], C.byref(got))
+    res = out[:, :got.value]
+    return (res, nclip.value) if return_clipped else res
