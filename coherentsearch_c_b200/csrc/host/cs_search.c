@@ -6,10 +6,12 @@
  * candidate arithmetic rounds like the reference's.
  */
 #include "coherent_search.h"
+#include "cs_b200.h"
 
 #include <errno.h>
 #include <fcntl.h>
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #include <sys/mman.h>
@@ -656,4 +658,100 @@ double cs_prep_pad_value(const float *x, long long n)
         avg += dev / ((double)(int)i + 1.0);
     }
     return avg;
+}
+
+/* ------------------------------------------------------------------ */
+/* SIGPROC filterbank header, third_party/presto/src/sigproc_fb.c      */
+/* ------------------------------------------------------------------ */
+/* one length-prefixed string (sigproc_fb.c get_string); -1 at end of file or
+ * on a length outside 1..79 */
+static int sp_string(FILE *f, char *out)
+{
+    int n;
+    if (fread(&n, sizeof(int), 1, f) != 1 || n < 1 || n > 79) return -1;
+    if (fread(out, 1, (size_t)n, f) != (size_t)n) return -1;
+    out[n] = '\0';
+    return 0;
+}
+
+/* The keywords read_filterbank_header (sigproc_fb.c:240-345) accepts, with
+ * the derived band edges of its spectra_info setup (:435-441).  Only what the
+ * device front end takes is accepted: 8-bit unsigned samples, one IF,
+ * channels stored highest frequency first (foff < 0).  The data offset is the
+ * position after HEADER_END.  Returns 0, or -1 with a message on stderr. */
+int cs_sigproc_read_header(const char *path, CsSigproc *h)
+{
+    char key[80];
+    memset(h, 0, sizeof(*h));
+    h->nifs = 1;
+    h->ibeam = 1;
+    FILE *f = fopen(path, "rb");
+    if (!f) {
+        fprintf(stderr, "Error: cannot open '%s': %s\n", path, strerror(errno));
+        return -1;
+    }
+    int ok = sp_string(f, key) == 0 && strcmp(key, "HEADER_START") == 0;
+    if (!ok) fprintf(stderr, "Error: %s: not a SIGPROC filterbank header\n", path);
+    int want_name = 0, want_raw = 0, done = 0;
+    while (ok && !done) {
+        if (sp_string(f, key) != 0) {
+            fprintf(stderr, "Error: %s: malformed SIGPROC header\n", path);
+            ok = 0;
+            break;
+        }
+        int iv = 0;
+        double dv = 0.0;
+#define RD(dst) (fread(&(dst), sizeof(dst), 1, f) == 1)
+        if (!strcmp(key, "HEADER_END")) done = 1;
+        else if (!strcmp(key, "source_name")) want_name = 1;
+        else if (!strcmp(key, "rawdatafile")) want_raw = 1;
+        else if (!strcmp(key, "tstart")) ok = RD(h->tstart);
+        else if (!strcmp(key, "tsamp")) ok = RD(h->tsamp);
+        else if (!strcmp(key, "fch1")) ok = RD(h->fch1);
+        else if (!strcmp(key, "foff")) ok = RD(h->foff);
+        else if (!strcmp(key, "src_raj")) ok = RD(h->src_raj);
+        else if (!strcmp(key, "src_dej")) ok = RD(h->src_dej);
+        else if (!strcmp(key, "az_start") || !strcmp(key, "za_start")) ok = RD(dv);
+        else if (!strcmp(key, "nchans")) ok = RD(h->nchans);
+        else if (!strcmp(key, "nbits")) ok = RD(h->nbits);
+        else if (!strcmp(key, "nifs")) ok = RD(h->nifs);
+        else if (!strcmp(key, "ibeam")) ok = RD(h->ibeam);
+        else if (!strcmp(key, "telescope_id")) ok = RD(h->telescope_id);
+        else if (!strcmp(key, "machine_id")) ok = RD(h->machine_id);
+        else if (!strcmp(key, "data_type") || !strcmp(key, "barycentric") ||
+                 !strcmp(key, "pulsarcentric") || !strcmp(key, "nsamples") ||
+                 !strcmp(key, "nbeams")) ok = RD(iv);
+        else if (!strcmp(key, "signed")) {
+            char c;
+            ok = fread(&c, 1, 1, f) == 1;
+            h->signedints = c;
+        }
+        else if (want_name) { snprintf(h->source_name, sizeof(h->source_name), "%s", key); want_name = 0; }
+        else if (want_raw) { snprintf(h->rawdatafile, sizeof(h->rawdatafile), "%s", key); want_raw = 0; }
+        else {
+            fprintf(stderr, "Error: %s: unknown SIGPROC header keyword '%s'\n", path, key);
+            ok = 0;
+        }
+#undef RD
+    }
+    if (!ok || !done) {
+        fclose(f);
+        return -1;
+    }
+    h->header_bytes = (long long)ftell(f);
+    struct stat stt;
+    const int sr = fstat(fileno(f), &stt);
+    fclose(f);
+    if (sr != 0) return -1;
+    if (h->nbits != 8 || h->nifs != 1 || h->nchans < 1 || !(h->foff < 0.0) ||
+        !(h->tsamp > 0.0) || h->signedints) {
+        fprintf(stderr, "Error: %s: the device front end takes 8-bit unsigned, one-IF "
+                        "filterbanks with descending channels (nbits %d, nifs %d, nchans %d, "
+                        "foff %g)\n", path, h->nbits, h->nifs, h->nchans, h->foff);
+        return -1;
+    }
+    h->nspectra = ((long long)stt.st_size - h->header_bytes) / h->nchans;
+    h->chanwid = fabs(h->foff);
+    h->lofreq = h->fch1 - (double)(h->nchans - 1) * h->chanwid;
+    return 0;
 }

@@ -228,3 +228,31 @@ def make_filterbank(spec: FilterbankSpec, chunk: int = 1 << 14) -> np.ndarray:
         np.clip(np.rint(x), 0, 255, out=x)
         out[t0:t0 + n] = x[:, ::-1].astype(np.uint8)
     return out
+
+
+def write_filterbank(path: str, raw: np.ndarray, spec: FilterbankSpec,
+                     source_name: str = "SYNTH", tstart: float = 60000.0) -> None:
+    """An 8-bit SIGPROC filterbank file of raw ([nspec][nchan], highest
+    frequency first) with the header keywords PRESTO reads
+    (third_party/presto/src/sigproc_fb.c:240-345): fch1 the highest channel,
+    foff = -chanwid."""
+    import struct
+
+    def s(x: str) -> bytes:
+        b = x.encode()
+        return struct.pack("<i", len(b)) + b
+
+    hdr = (s("HEADER_START") + s("source_name") + s(source_name) +
+           s("telescope_id") + struct.pack("<i", 0) + s("machine_id") + struct.pack("<i", 0) +
+           s("data_type") + struct.pack("<i", 1) +
+           s("fch1") + struct.pack("<d", spec.lofreq + (spec.nchan - 1) * spec.chanwid) +
+           s("foff") + struct.pack("<d", -spec.chanwid) +
+           s("nchans") + struct.pack("<i", spec.nchan) + s("nbits") + struct.pack("<i", 8) +
+           s("tstart") + struct.pack("<d", tstart) + s("tsamp") + struct.pack("<d", spec.dt) +
+           s("nifs") + struct.pack("<i", 1) + s("HEADER_END"))
+    raw = np.ascontiguousarray(raw, dtype=np.uint8)
+    if raw.ndim != 2 or raw.shape[1] != spec.nchan:
+        raise ValueError("raw must be [nspec][nchan] uint8")
+    with open(path, "wb") as f:
+        f.write(hdr)
+        f.write(raw.tobytes())

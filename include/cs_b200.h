@@ -158,6 +158,23 @@ void cs_ducy_free(CsDucy *d);
 int cs_clip_count(const uint8_t *d_raw, long long nspec, int nchan, int L, float clip_sigma,
                   long long *nclipped, uint8_t *d_flags, void *stream, int device);
 
+/* ---- SIGPROC filterbank header (in libcoherent_search.so) --------------
+ * The header read_filterbank_header parses (third_party/presto/
+ * src/sigproc_fb.c:240-345) and the band edges PRESTO derives from it
+ * (:435-441): lofreq = fch1 - (nchans - 1) * |foff| (the centre of the lowest
+ * channel), chanwid = |foff|.  header_bytes is where the [nspectra][nchans]
+ * 8-bit samples start.  Returns 0, or -1 (message on stderr) for a file the
+ * device front end cannot take (not 8-bit unsigned, several IFs, ascending
+ * channels). */
+typedef struct {
+    int nchans, nbits, nifs, ibeam, telescope_id, machine_id, signedints;
+    double tstart, tsamp, fch1, foff, src_raj, src_dej;
+    char source_name[80], rawdatafile[80];
+    long long header_bytes, nspectra;
+    double lofreq, chanwid;
+} CsSigproc;
+int cs_sigproc_read_header(const char *path, CsSigproc *h);
+
 /* The value prepsubband pads every DM series with: PRESTO's running mean
  * (update_stats) of DM 0's n output samples.  In libcoherent_search.so. */
 double cs_prep_pad_value(const float *x, long long n);

@@ -47,7 +47,7 @@ def test_host_library_exports_reference_api():
             "analytic_sigma", "boxcar_shape", "candlist_init", "candlist_free",
             "candlist_push", "remove_duplicates", "remove_harmonics", "write_candidates",
             "measure_ducy", "search_file", "search_cache_free", "fftfile_open",
-            "fftfile_close", "inf_read"}
+            "fftfile_close", "inf_read", "cs_prep_pad_value", "cs_sigproc_read_header"}
     assert want <= exp, sorted(want - exp)
 
 
