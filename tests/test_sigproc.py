@@ -85,8 +85,19 @@ def test_front_end_from_file(gpu_ready, tmp_path):
     numout = 1 << 15
     ref = rb.ref_dedisp_run(np.asarray(data), t.nsub, t.idispdt, t.offsets,
                             t.spectra_per_subint, t.blocks_per_read, numout)
+    d = torch.from_numpy(np.array(data)).cuda()
+    # this pulsar is nearly undispersed over 64 MHz, so prepsubband's default
+    # 6-sigma clip would cut it: the front end says so, with the reference's count
+    _, nclip = rb.ref_dedisp_run(np.asarray(data), t.nsub, t.idispdt, t.offsets,
+                                 t.spectra_per_subint, t.blocks_per_read, numout,
+                                 clip_sigma=6.0, return_clipped=True)
+    assert nclip > 0
     with PrepSearch(t, h["nspectra"], numout, h["tsamp"], Options(blocksize=4096)) as ps:
-        d = torch.from_numpy(np.ascontiguousarray(data)).cuda()
+        assert ps.dd.clip_count(d.data_ptr(), h["nspectra"], 6.0) == nclip
+        with pytest.raises(RuntimeError, match="clip"):
+            ps.dedisperse(d.data_ptr(), h["nspectra"])
+    with PrepSearch(t, h["nspectra"], numout, h["tsamp"], Options(blocksize=4096),
+                    clip_sigma=0) as ps:                       # -noclip
         ps.dedisperse(d.data_ptr(), h["nspectra"])
         pad = np.float32(running_mean(ref[0]))
         for dm in (0, 5, 11):
