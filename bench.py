@@ -667,6 +667,11 @@ def run_prep(args):
     value = world * trials / (ms * 1e-3)
     hbm_peak, tc_peak, peak_kind = load_peaks()
     kms = statistics.mean(search_ms)
+    # the default 6-sigma clip check, timed on its own (it runs inside each step)
+    torch.cuda.synchronize()
+    c0 = time.perf_counter()
+    ps.dd.clip_count(raw.data_ptr(), spec.nspec, ps.clip_sigma or 6.0, stream.cuda_stream)
+    clip_ms = 1e3 * (time.perf_counter() - c0)
     dft_tflops = trials * DFT_FLOP_PER_TRIAL / (kms * 1e-3) / 1e12
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -689,7 +694,8 @@ def run_prep(args):
                      "algorithmic": f"{DFT_FLOP_PER_TRIAL:.0f} DFT flop/trial x {total} trials "
                                     f"x {t.ndm} DMs"},
         "stages_ms": {"dedisp": statistics.mean(dd_ms), "search_kernels": kms,
-                      "rest": ms - statistics.mean(dd_ms) - kms},
+                      "rest": ms - statistics.mean(dd_ms) - kms,
+                      "clip_check": clip_ms, "steps": [round(x, 2) for x in times]},
         "clocks": clk.summary(),
         "candidates": ncand,
     }

@@ -24,9 +24,13 @@
  *                    sort gives (kept candidates never tie in frequency:
  *                    equal frequencies are related with m = n = 1).
  *
- * The sorts are CUB radix sorts (stable) on the keys' bit patterns (r and
- * freq are positive, so their IEEE bits order like the values; the metric
- * sort uses CUB's floating-point key handling).  The greedy pass runs in one
+ * Ordering without a sort on r: within one decimation slot, r (and freq)
+ * rises strictly with the trial index, so a CUB radix sort on (slot, chunk,
+ * j) lines every slot up in r order, and a merge places each candidate at
+ * its own position in its slot plus, for every other slot, the number of
+ * candidates there that come before it in (r, chunk, slot, j) order (a
+ * binary search): the stable r order of the (chunk, slot, j) base order.
+ * The metrics are FP32 values, so the metric sort uses 32-bit float keys.  The greedy pass runs in one
  * CTA: for each kept candidate, in metric order, the threads mark every later
  * candidate it is related to; a candidate is kept when no earlier kept one
  * marked it, as in the host loop.  The FP64 expressions are the host's.
@@ -54,10 +58,11 @@ struct SlotInfo {
 };
 
 __global__ void harvest_kernel(const CsRec *recs, unsigned n, const CsChunk *chunks,
-                               SlotInfo si, int nslot, int nprof, double r_lo, double lodr,
-                               double nyq, double T, double thr, uint64_t *key, unsigned *idx,
+                               long long nchunks, SlotInfo si, int nslot, int nprof,
+                               double r_lo, double lodr, double nyq, double T, double thr,
+                               uint64_t *key, uint64_t *bkey, int *slot_of, unsigned *idx,
                                double *r, double *freq, double *metric, int *nharm,
-                               unsigned *nvalid)
+                               unsigned *nvalid, unsigned *slot_cnt)
 {
     const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -74,8 +79,13 @@ __global__ void harvest_kernel(const CsRec *recs, unsigned n, const CsChunk *chu
     }
     idx[i] = i;
     if (ok) {
-        key[i] = ((uint64_t)rc.chunk * (uint64_t)nslot + (uint64_t)rc.slot) * (uint64_t)nprof +
+        /* sort key (slot, chunk, j); tie-break key (chunk, slot, j), the base order */
+        key[i] = ((uint64_t)rc.slot * (uint64_t)nchunks + (uint64_t)rc.chunk) * (uint64_t)nprof +
                  (uint64_t)rc.j;
+        bkey[i] = ((uint64_t)rc.chunk * (uint64_t)nslot + (uint64_t)rc.slot) * (uint64_t)nprof +
+                  (uint64_t)rc.j;
+        slot_of[i] = rc.slot;
+        atomicAdd(&slot_cnt[rc.slot], 1u);
         r[i] = rsel;
         freq[i] = rsel / T;
         metric[i] = m;
@@ -83,6 +93,8 @@ __global__ void harvest_kernel(const CsRec *recs, unsigned n, const CsChunk *chu
         atomicAdd(nvalid, 1u);
     } else {
         key[i] = ~0ull;                 /* after every valid record */
+        bkey[i] = ~0ull;
+        slot_of[i] = 0;
         r[i] = INFINITY;
         freq[i] = INFINITY;
         metric[i] = -INFINITY;
@@ -90,12 +102,37 @@ __global__ void harvest_kernel(const CsRec *recs, unsigned n, const CsChunk *chu
     }
 }
 
-/* bits of a positive double (or +inf) in the order of the sort */
-__global__ void gather_bits_kernel(const unsigned *order, const double *v, unsigned n,
-                                   uint64_t *bits)
+__global__ void slot_starts_kernel(const unsigned *cnt, int nslot, unsigned *start)
+{
+    unsigned acc = 0;
+    for (int s = 0; s < nslot; s++) { start[s] = acc; acc += cnt[s]; }
+}
+
+/* order1 holds the valid records grouped by slot, each group in trial order
+ * (so in strictly rising v); out receives them in (v, base key) order */
+__global__ void merge_kernel(const unsigned *order1, const unsigned *nv, const int *slot_of,
+                             const uint64_t *bkey, const double *v, const unsigned *start,
+                             const unsigned *cnt, int nslot, unsigned *out)
 {
     const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) bits[i] = (uint64_t)__double_as_longlong(v[order[i]]);
+    if (i >= *nv) return;
+    const unsigned x = order1[i];
+    const int s = slot_of[x];
+    const double vx = v[x];
+    const uint64_t bx = bkey[x];
+    unsigned rank = i - start[s];
+    for (int t = 0; t < nslot; t++) {
+        if (t == s || cnt[t] == 0) continue;
+        unsigned lo = start[t], hi = start[t] + cnt[t], a = lo, b = hi;
+        while (a < b) {
+            const unsigned mid = (a + b) >> 1;
+            if (v[order1[mid]] < vx) a = mid + 1; else b = mid;
+        }
+        unsigned c = a - lo;
+        if (a < hi && v[order1[a]] == vx && bkey[order1[a]] < bx) c++;
+        rank += c;
+    }
+    out[rank] = x;
 }
 
 /* run starts of remove_duplicates over the first nv of the r-sorted list
@@ -138,11 +175,11 @@ __global__ void copy_count_kernel(const unsigned *src, unsigned *dst)
 
 /* descending-sort keys; entries past m sort after every real one */
 __global__ void gather_metric_kernel(const unsigned *list, const double *metric, unsigned n,
-                                     const unsigned *m, double *key, unsigned *pos)
+                                     const unsigned *m, float *key, unsigned *pos)
 {
     const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    key[i] = i < *m ? metric[list[i]] : -INFINITY;
+    key[i] = i < *m ? (float)metric[list[i]] : -INFINITY;     /* FP32 values: exact */
     pos[i] = i;
 }
 
@@ -225,14 +262,18 @@ struct CsCollapse {
     size_t cap;                     /* records */
     uint64_t *key[2];
     unsigned *idx[2];
+    uint64_t *bkey;
+    int *slot_of;
+    unsigned *merged;
     double *r, *freq, *metric;
     int *nharm;
     unsigned *flag, *runid, *list;
-    double *mkey[2];
+    float *mkey[2];
     unsigned *mpos[2];
     unsigned char *removed, *keep;
     Candidate *out;
-    unsigned *counters;             /* device: nvalid, runs, kept */
+    unsigned *counters;             /* device: nvalid, runs, kept; then per-slot counts
+                                       and starts (CS_MAX_SLOT each) */
     unsigned *h_counters;           /* pinned */
     Candidate *h_out;               /* pinned */
     size_t h_out_cap;
@@ -247,6 +288,8 @@ static void collapse_release_buffers(CsCollapse *w)
         cudaFree(w->key[b]); cudaFree(w->idx[b]); cudaFree(w->mkey[b]); cudaFree(w->mpos[b]);
         w->key[b] = nullptr; w->idx[b] = nullptr; w->mkey[b] = nullptr; w->mpos[b] = nullptr;
     }
+    cudaFree(w->bkey); cudaFree(w->slot_of); cudaFree(w->merged);
+    w->bkey = nullptr; w->slot_of = nullptr; w->merged = nullptr;
     cudaFree(w->r); cudaFree(w->freq); cudaFree(w->metric); cudaFree(w->nharm);
     cudaFree(w->flag); cudaFree(w->runid); cudaFree(w->list);
     cudaFree(w->removed); cudaFree(w->keep); cudaFree(w->out); cudaFree(w->temp);
@@ -270,9 +313,12 @@ static cudaError_t collapse_reserve(CsCollapse *w, size_t n)
     for (int b = 0; b < 2; b++) {
         AL(w->key[b], c * sizeof(uint64_t));
         AL(w->idx[b], c * sizeof(unsigned));
-        AL(w->mkey[b], c * sizeof(double));
+        AL(w->mkey[b], c * sizeof(float));
         AL(w->mpos[b], c * sizeof(unsigned));
     }
+    AL(w->bkey, c * sizeof(uint64_t));
+    AL(w->slot_of, c * sizeof(int));
+    AL(w->merged, c * sizeof(unsigned));
     AL(w->r, c * sizeof(double));
     AL(w->freq, c * sizeof(double));
     AL(w->metric, c * sizeof(double));
@@ -283,14 +329,14 @@ static cudaError_t collapse_reserve(CsCollapse *w, size_t n)
     AL(w->removed, c);
     AL(w->keep, c);
     AL(w->out, c * sizeof(Candidate));
-    if (!w->counters) AL(w->counters, 4 * sizeof(unsigned));
+    if (!w->counters) AL(w->counters, (4 + 2 * CS_MAX_SLOT) * sizeof(unsigned));
 #undef AL
     if (e != cudaSuccess) return e;
     /* the largest CUB scratch any step needs at this capacity */
     size_t t1 = 0, t2 = 0, t3 = 0;
     cub::DoubleBuffer<uint64_t> kb(w->key[0], w->key[1]);
     cub::DoubleBuffer<unsigned> ib(w->idx[0], w->idx[1]);
-    cub::DoubleBuffer<double> mb(w->mkey[0], w->mkey[1]);
+    cub::DoubleBuffer<float> mb(w->mkey[0], w->mkey[1]);
     cub::DoubleBuffer<unsigned> pb(w->mpos[0], w->mpos[1]);
     e = cub::DeviceRadixSort::SortPairs(nullptr, t1, kb, ib, (int)c);
     if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairsDescending(nullptr, t2, mb, pb, (int)c);
@@ -353,33 +399,31 @@ int cs_collapse_enqueue(CsCollapse *w, const CsRec *recs, unsigned n, const CsCh
         return -1;
     }
     unsigned *nv = w->counters, *m = w->counters + 1, *nout = w->counters + 2;
-    e = cudaMemsetAsync(w->counters, 0, 4 * sizeof(unsigned), st);
+    e = cudaMemsetAsync(w->counters, 0, (4 + 2 * CS_MAX_SLOT) * sizeof(unsigned), st);
+    unsigned *slot_cnt = w->counters + 4, *slot_start = w->counters + 4 + CS_MAX_SLOT;
     if (e == cudaSuccess) {
-        cl::harvest_kernel<<<g, cl::NT, 0, st>>>(recs, n, chunks, si, nslot, nprof, r_lo, lodr,
-                                                 N / 2.0, T, threshold, w->key[0], w->idx[0],
-                                                 w->r, w->freq, w->metric, w->nharm, nv);
+        cl::harvest_kernel<<<g, cl::NT, 0, st>>>(recs, n, chunks, nchunks, si, nslot, nprof,
+                                                 r_lo, lodr, N / 2.0, T, threshold, w->key[0],
+                                                 w->bkey, w->slot_of, w->idx[0], w->r, w->freq,
+                                                 w->metric, w->nharm, nv, slot_cnt);
         e = cudaGetLastError();
     }
-    /* the base order: (chunk, slot, j); invalid records (all-ones key) last */
+    /* every slot's records in trial order; invalid records (all-ones key) last */
     cub::DoubleBuffer<uint64_t> kb(w->key[0], w->key[1]);
     cub::DoubleBuffer<unsigned> ib(w->idx[0], w->idx[1]);
     if (e == cudaSuccess) {
         tb = w->temp_bytes;
         e = cub::DeviceRadixSort::SortPairs(w->temp, tb, kb, ib, (int)n, 0, end_bit, st);
     }
-    /* then stably by r (remove) or by frequency (no remove); +inf last */
-    cub::DoubleBuffer<uint64_t> kb2(kb.Alternate(), kb.Current());
-    cub::DoubleBuffer<unsigned> ib2(ib.Current(), ib.Alternate());
+    /* merged into stable r order (remove) or stable frequency order */
     if (e == cudaSuccess) {
-        cl::gather_bits_kernel<<<g, cl::NT, 0, st>>>(ib.Current(), remove ? w->r : w->freq, n,
-                                                     kb2.Current());
+        cl::slot_starts_kernel<<<1, 1, 0, st>>>(slot_cnt, nslot, slot_start);
+        cl::merge_kernel<<<g, cl::NT, 0, st>>>(ib.Current(), nv, w->slot_of, w->bkey,
+                                               remove ? w->r : w->freq, slot_start, slot_cnt,
+                                               nslot, w->merged);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess) {
-        tb = w->temp_bytes;
-        e = cub::DeviceRadixSort::SortPairs(w->temp, tb, kb2, ib2, (int)n, 0, 64, st);
-    }
-    order = ib2.Current();
+    order = w->merged;
     if (remove) {
         if (e == cudaSuccess) {
             cl::run_flags_kernel<<<g, cl::NT, 0, st>>>(order, w->r, n, nv, dr_tol, w->flag);
@@ -409,11 +453,11 @@ int cs_collapse_enqueue(CsCollapse *w, const CsRec *recs, unsigned n, const CsCh
                                                            w->mpos[0]);
             e = cudaGetLastError();
         }
-        cub::DoubleBuffer<double> mb(w->mkey[0], w->mkey[1]);
+        cub::DoubleBuffer<float> mb(w->mkey[0], w->mkey[1]);
         cub::DoubleBuffer<unsigned> pb(w->mpos[0], w->mpos[1]);
         if (e == cudaSuccess) {
             tb = w->temp_bytes;
-            e = cub::DeviceRadixSort::SortPairsDescending(w->temp, tb, mb, pb, (int)n, 0, 64, st);
+            e = cub::DeviceRadixSort::SortPairsDescending(w->temp, tb, mb, pb, (int)n, 0, 32, st);
         }
         if (e == cudaSuccess) {
             cl::greedy_kernel<<<1, 1024, 0, st>>>(listp, pb.Current(), w->r, m, numharm,

@@ -30,10 +30,11 @@ def running_mean(x: np.ndarray) -> float:
 class PrepSearch:
     """Dedisperse a filterbank and search every DM series on one GPU.
 
-    Three search sessions of the one geometry take the DMs in turn.  At DM i
-    the host queues DM i's spectrum (prep stream) and search, then DM i-1's
-    collapse, then waits for DM i-2's list, so the GPU always has the next
-    search queued behind the collapse work.  Without collapsing, DM i-1's raw
+    Four search sessions of the one geometry take the DMs in turn.  At DM i
+    the host queues DM i's spectrum (prep stream) and search, then DM i-2's
+    collapse (which first waits for DM i-2's search), then takes DM i-3's
+    list, so two searches stay queued ahead of the host and a host stall of a
+    few milliseconds does not idle the GPU.  Without collapsing, DM i-1's raw
     records are read back while DM i is searched."""
 
     def __init__(self, tables: DedispTables, nspec: int, numout: int, dt: float,
@@ -54,7 +55,7 @@ class PrepSearch:
         self.out = torch.empty((tables.ndm, self.stride), dtype=torch.float32, device=self.dev)
         self.stream = torch.cuda.Stream(device=self.dev)
         self.spec = SpectrumMaker(self.N, dt, device=device)
-        self.sessions = [Session(self.N, dt, self.opts, device=device) for _ in range(3)]
+        self.sessions = [Session(self.N, dt, self.opts, device=device) for _ in range(4)]
         self.ses = self.sessions[0]
         self.pad_value = None
         # prepsubband clips at 6 sigma unless told -noclip (0 here): the device
@@ -131,17 +132,17 @@ class PrepSearch:
             self._spectrum(d, ses)
             ses.enqueue(None, threshold, after_stream=self.stream.cuda_stream)
             if collapse:
-                if i >= 1:
-                    start_collapse(i - 1)
                 if i >= 2:
-                    finish(i - 2)
+                    start_collapse(i - 2)
+                if i >= 3:
+                    finish(i - 3)
             elif i >= 1:
                 finish(i - 1)
         n = len(dms)
         if collapse:
-            if n >= 1:
-                start_collapse(n - 1)
             for j in range(max(0, n - 2), n):
+                start_collapse(j)
+            for j in range(max(0, n - 3), n):
                 finish(j)
         elif n >= 1:
             finish(n - 1)
