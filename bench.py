@@ -976,6 +976,119 @@ def serve_reference_gpu(reqs, served_results, served_rate, limit=60):
                       "requests back to back (a lower bound on its latency under load)"}
 
 
+def run_series(args):
+    """The small configuration end to end: an N = 2^20 float32 series (7.3 Hz
+    pulsar, 5 % duty) -> realfft + rednoise on the GPU -> search (nharms 60,
+    m 16, blocksize 2048, threshold 8) -> search_file's collapsed list."""
+    import torch
+    from coherentsearch_c_b200 import synth
+    from coherentsearch_c_b200.search import Options, Session
+    from coherentsearch_c_b200.spectrum import SpectrumMaker
+    torch.cuda.set_device(0)
+    dev = "cuda:0"
+    spec = synth.config_small()
+    x = synth.make_series(spec).astype(np.float32)
+    N, dt = x.size, spec.dt
+    opts = Options(nharms=60, m=16, blocksize=2048, threshold=8.0)
+    ses = Session(N, dt, opts)
+    sm = SpectrumMaker(N, dt)
+    total = ses.total
+    stream = torch.cuda.Stream(device=dev)
+    d_x = torch.from_numpy(x).to(dev)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        sm.run_device(d_x.data_ptr(), ses.device_amps_ptr(), stream.cuda_stream)
+        ses.enqueue(None, after_stream=stream.cuda_stream)
+        out, kms, rc = ses.collect_collapsed()
+        if rc == 1:
+            ses.enqueue(None)
+            out, kms, rc = ses.collect_collapsed()
+        return out, kms
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    times, kern = [], []
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            out, kms = step()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            kern.append(kms)
+        # end to end: the series from pinned host memory, candidates back
+        h_x = torch.empty(N, dtype=torch.float32, pin_memory=True)
+        h_x.numpy()[:] = x
+        e2e = []
+        for _ in range(max(3, args.steps // 2)):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            with torch.cuda.stream(stream):
+                d_x.copy_(h_x, non_blocking=True)
+            out, _ = step()
+            e1.record(stream)
+            e1.synchronize()
+            e2e.append(e0.elapsed_time(e1))
+    ms = statistics.mean(times)
+    kms = statistics.mean(kern)
+    hbm_peak, tc_peak, peak_kind = load_peaks()
+    dft = total * DFT_FLOP_PER_TRIAL / (kms * 1e-3) / 1e12
+    line = {
+        "metric": METRIC, "value": total / (ms * 1e-3), "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "small configuration: N=2^20 f32 series, dt 64 us, 7.3 Hz "
+                               "pulsar (5 % duty, folded S/N ~15) in white noise; realfft + "
+                               "rednoise on the GPU, search nharms 60, m 16, blocksize 2048, "
+                               "lobin 100, 0.1-125 Hz, hidr 0.5, threshold 8, collapsed",
+                   "trials": total, "l2": "flushed (512 MiB write) before each timed step",
+                   "parallelism": "replicas1"},
+        "e2e": {"value": total / (statistics.mean(e2e) * 1e-3), "unit": UNIT,
+                "h2d_bytes_per_step": int(x.nbytes), "d2h_bytes_per_step": int(out.nbytes)},
+        "gpu_launches": 15 * args.steps,
+        "roofline": {"bound": "tensor", "achieved": dft, "peak": tc_peak, "unit": "TFLOP/s",
+                     "frac": dft / tc_peak, "traffic": None,
+                     "kernel": "search_ws60" if ses.info().kernel == 1 else "cs_search_kernel",
+                     "kernel_ms": kms, "peak_kind": f"bf16 dense, {peak_kind}"},
+        "candidates": int(out.size),
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import refbind as rb
+        cores = os.cpu_count() or 1
+        rb.ref_lib()
+        rb.pin_ref_threads(cores)
+        ref = rb.ref_search(rb.ref_spectrum(x, dt), N, dt, opts)
+        reps, t0 = 0, time.perf_counter()
+        while reps < 40:
+            rb.ref_search(rb.ref_spectrum(x, dt), N, dt, opts)
+            reps += 1
+            if time.perf_counter() - t0 >= args.cpu_seconds:
+                break
+        rate = total * reps / (time.perf_counter() - t0)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
+                                "sample": f"{reps} runs of realfft + rednoise + search_file "
+                                          f"(OpenMP, {cores} threads) on the same series"}
+        line["candidates_reference"] = int(ref.size)
+        line["candidates_common"] = len(set(zip(np.round(ref["r"], 9), ref["nharm"])) &
+                                        set(zip(np.round(out["r"], 9), out["nharm"])))
+    print(json.dumps(line))
+    ses.close()
+    sm.close()
+    return 0
+
+
 def profiled_traffic(kernel, total):
     """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
     summary profiles/<kernel>_n23_traffic.md, a line `bytes_per_launch: B`
@@ -1006,12 +1119,13 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="search",
-                    choices=["search", "dedisp", "sweep", "serve", "prep"],
+                    choices=["search", "dedisp", "sweep", "serve", "prep", "series"],
                     help="search: the coherent search (headline); dedisp: subband "
                          "dedispersion of the 8-bit filterbank workload; sweep: batched "
                          "search of a list of uneven-length files; serve: a Poisson "
                          "stream of requests through the request loop; prep: the raw-data "
-                         "front end, filterbank -> dedispersion -> search of every DM")
+                         "front end, filterbank -> dedispersion -> search of every DM; "
+                         "series: the small configuration from a time series")
     ap.add_argument("--files", type=int, default=256, help="sweep: number of files")
     ap.add_argument("--slots", type=int, default=3, help="sweep/serve: batch slots")
     ap.add_argument("--requests", type=int, default=800, help="serve: requests")
@@ -1048,6 +1162,13 @@ def main():
                               "object of its own line"}))
             return 0
         return run_dedisp(args)
+    if args.workload == "series":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the small configuration's reference arm is the cpu_baseline "
+                              "object of its own line"}))
+            return 0
+        return run_series(args)
     if args.workload == "prep":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable":

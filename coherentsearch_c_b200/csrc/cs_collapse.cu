@@ -11,7 +11,8 @@
  *                    cs_gpu_session_run returns;
  *   remove           remove_duplicates (src/candidate.c:98-128): a stable
  *                    sort by r, runs whose consecutive r differ by at most
- *                    dr_tol, the first member of largest metric of each run;
+ *                    dr_tol, the first member of largest metric of each run
+ *                    (a segmented argmax by 64-bit atomicMax);
  *                    the result is in r order, which is also its frequency
  *                    order (freq = r / T, and two members of one list never
  *                    tie in freq without falling into one run);
@@ -145,21 +146,35 @@ __global__ void run_flags_kernel(const unsigned *order, const double *r, unsigne
     flag[i] = i < *nv && (i == 0 || r[order[i]] - r[order[i - 1]] > drtol) ? 1u : 0u;
 }
 
-/* each run start scans its run: the first member of largest metric */
-__global__ void run_pick_kernel(const unsigned *order, const double *metric,
-                                const unsigned *flag, const unsigned *runid,
-                                const unsigned *nv, unsigned *out)
+/* the first member of largest metric of each run, as a segmented argmax:
+ * every candidate offers (metric, earliest position) to its run with one
+ * 64-bit atomicMax.  The metrics are FP32 values, so their float bits (made
+ * order-preserving) compare like the doubles the host compares. */
+static __device__ __forceinline__ uint32_t ordered_bits(float f)
+{
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+__global__ void run_offer_kernel(const unsigned *order, const double *metric,
+                                 const unsigned *flag, const unsigned *runid,
+                                 const unsigned *nv, unsigned long long *best)
 {
     const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-    const unsigned n = *nv;
-    if (i >= n || !flag[i]) return;
-    unsigned best = order[i];
-    double bm = metric[best];
-    for (unsigned j = i + 1; j < n && !flag[j]; j++) {
-        const unsigned c = order[j];
-        if (metric[c] > bm) { bm = metric[c]; best = c; }
-    }
-    out[runid[i]] = best;
+    if (i >= *nv) return;
+    const unsigned run = runid[i] + flag[i] - 1u;
+    const unsigned long long key =
+        ((unsigned long long)ordered_bits((float)metric[order[i]]) << 32) |
+        (unsigned long long)(0xFFFFFFFFu - i);
+    atomicMax(&best[run], key);
+}
+
+__global__ void run_take_kernel(const unsigned *order, const unsigned long long *best,
+                                unsigned n, const unsigned *m, unsigned *out)
+{
+    const unsigned r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n || r >= *m) return;
+    out[r] = order[0xFFFFFFFFu - (unsigned)(best[r] & 0xFFFFFFFFull)];
 }
 
 __global__ void count_runs_kernel(const unsigned *flag, const unsigned *runid, unsigned n,
@@ -433,10 +448,14 @@ int cs_collapse_enqueue(CsCollapse *w, const CsRec *recs, unsigned n, const CsCh
             tb = w->temp_bytes;
             e = cub::DeviceScan::ExclusiveSum(w->temp, tb, w->flag, w->runid, (int)n, st);
         }
+        /* the key buffers are free once the merge has run: best-of-run slots */
+        unsigned long long *best = reinterpret_cast<unsigned long long *>(w->key[0]);
+        if (e == cudaSuccess) e = cudaMemsetAsync(best, 0, (size_t)n * sizeof(uint64_t), st);
         if (e == cudaSuccess) {
-            cl::run_pick_kernel<<<g, cl::NT, 0, st>>>(order, w->metric, w->flag, w->runid, nv,
-                                                      w->list);
             cl::count_runs_kernel<<<1, 1, 0, st>>>(w->flag, w->runid, n, m);
+            cl::run_offer_kernel<<<g, cl::NT, 0, st>>>(order, w->metric, w->flag, w->runid, nv,
+                                                       best);
+            cl::run_take_kernel<<<g, cl::NT, 0, st>>>(order, best, n, m, w->list);
             e = cudaGetLastError();
         }
         listp = w->list;
