@@ -670,7 +670,10 @@ def run_prep(args):
     # the default 6-sigma clip check, timed on its own (it runs inside each step)
     torch.cuda.synchronize()
     c0 = time.perf_counter()
-    ps.dd.clip_count(raw.data_ptr(), spec.nspec, ps.clip_sigma or 6.0, stream.cuda_stream)
+    scr = getattr(ps, "_clip_scratch", None)
+    ps.dd.clip_count(raw.data_ptr(), spec.nspec, ps.clip_sigma or 6.0, stream.cuda_stream,
+                     scr.data_ptr() if scr is not None else None,
+                     scr.numel() if scr is not None else 0)
     clip_ms = 1e3 * (time.perf_counter() - c0)
     dft_tflops = trials * DFT_FLOP_PER_TRIAL / (kms * 1e-3) / 1e12
     line = {

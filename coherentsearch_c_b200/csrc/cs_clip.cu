@@ -180,9 +180,30 @@ __global__ void decide_kernel(const int *zdm, long long n, int L, const float *r
 
 }  // namespace ck
 
+/* scratch layout: zero-DM sums, block statistics, running values, count */
+static size_t clip_layout(long long nspec, int L, size_t off[5])
+{
+    const long long nblocks = nspec / L, n = nblocks * L;
+    size_t o = 0;
+    auto take = [&](size_t bytes) { const size_t at = o; o = (o + bytes + 255) & ~(size_t)255; return at; };
+    off[0] = take((size_t)n * sizeof(int));
+    off[1] = take((size_t)nblocks * sizeof(ck::BlockStats));
+    off[2] = take((size_t)nblocks * sizeof(float));
+    off[3] = take((size_t)nblocks * sizeof(float));
+    off[4] = take(sizeof(unsigned long long));
+    return o;
+}
+
+CS_EXPORT size_t cs_clip_scratch_bytes(long long nspec, int L)
+{
+    if (nspec < 0 || L < 1) return 0;
+    size_t off[5];
+    return clip_layout(nspec, L, off);
+}
+
 CS_EXPORT int cs_clip_count(const uint8_t *d_raw, long long nspec, int nchan, int L,
                             float clip_sigma, long long *nclipped, uint8_t *d_flags,
-                            void *stream, int device)
+                            void *d_scratch, size_t scratch_bytes, void *stream, int device)
 {
     if (!nclipped || nchan < 1 || L < 1 || L > ck::MAX_L || nspec < 0) return -1;
     *nclipped = 0;
@@ -195,15 +216,22 @@ CS_EXPORT int cs_clip_count(const uint8_t *d_raw, long long nspec, int nchan, in
     int P2 = 1;
     while (P2 < L) P2 <<= 1;
     const size_t smem = (size_t)(L + P2) * sizeof(int);
-    int *zdm = nullptr;
-    ck::BlockStats *bs = nullptr;
-    float *ravg = nullptr, *trig = nullptr;
-    unsigned long long *cnt = nullptr, hcnt = 0;
-    cudaError_t e = cudaMalloc((void **)&zdm, (size_t)n * sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc((void **)&bs, (size_t)nblocks * sizeof(ck::BlockStats));
-    if (e == cudaSuccess) e = cudaMalloc((void **)&ravg, (size_t)nblocks * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc((void **)&trig, (size_t)nblocks * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc((void **)&cnt, sizeof(unsigned long long));
+    size_t off[5];
+    const size_t need = clip_layout(nspec, L, off);
+    cudaError_t e = cudaSuccess;
+    char *base = (char *)d_scratch;
+    const bool own = d_scratch == nullptr;
+    if (own) {
+        e = cudaMalloc((void **)&base, need);
+    } else if (scratch_bytes < need || ((uintptr_t)d_scratch & 255)) {
+        fprintf(stderr, "Error: cs_clip_count: scratch of %zu bytes (256-byte aligned) needed\n",
+                need);
+        return -1;
+    }
+    int *zdm = (int *)(base + off[0]);
+    ck::BlockStats *bs = (ck::BlockStats *)(base + off[1]);
+    float *ravg = (float *)(base + off[2]), *trig = (float *)(base + off[3]);
+    unsigned long long *cnt = (unsigned long long *)(base + off[4]), hcnt = 0;
     if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st);
     if (e == cudaSuccess && smem > 48 * 1024)
         e = cudaFuncSetAttribute((const void *)ck::block_kernel,
@@ -222,11 +250,7 @@ CS_EXPORT int cs_clip_count(const uint8_t *d_raw, long long nspec, int nchan, in
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(&hcnt, cnt, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    cudaFree(zdm);
-    cudaFree(bs);
-    cudaFree(ravg);
-    cudaFree(trig);
-    cudaFree(cnt);
+    if (own) cudaFree(base);
     if (e != cudaSuccess) {
         fprintf(stderr, "Error: cs_clip_count: %s\n", cudaGetErrorString(e));
         return -1;

@@ -105,14 +105,20 @@ class Dedisperser:
             raise RuntimeError("cs_dedisp_run_device failed (see stderr)")
         return got.value
 
+    def clip_scratch_bytes(self, nspec: int) -> int:
+        return int(self.lib.cs_clip_scratch_bytes(nspec, self.t.spectra_per_subint))
+
     def clip_count(self, d_raw: int, nspec: int, clip_sigma: float = 6.0,
-                   stream: int | None = None) -> int:
+                   stream: int | None = None, scratch: int | None = None,
+                   scratch_bytes: int = 0) -> int:
         """cs_clip_count: the spectra prepsubband's -clip clip_sigma would
         replace in this filterbank (0: the unclipped output is the clipped
-        run's)."""
+        run's).  scratch: a device buffer of clip_scratch_bytes(nspec) bytes
+        kept across calls (None: the call allocates its own)."""
         n = C.c_longlong(0)
         rc = self.lib.cs_clip_count(d_raw, nspec, self.t.nchan, self.t.spectra_per_subint,
-                                    float(clip_sigma), C.byref(n), None, stream, self.device)
+                                    float(clip_sigma), C.byref(n), None, scratch,
+                                    scratch_bytes, stream, self.device)
         if rc != 0:
             raise RuntimeError("cs_clip_count failed (see stderr)")
         return n.value

@@ -188,8 +188,11 @@ def declare_gpu_api(lib: C.CDLL) -> C.CDLL:
                                        C.c_void_p, C.c_longlong, P(C.c_double), C.c_void_p]
     lib.cs_ducy_run_device.restype = C.c_int
     lib.cs_ducy_free.argtypes = [C.c_void_p]
+    lib.cs_clip_scratch_bytes.argtypes = [C.c_longlong, C.c_int]
+    lib.cs_clip_scratch_bytes.restype = C.c_size_t
     lib.cs_clip_count.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_float,
-                                  P(C.c_longlong), C.c_void_p, C.c_void_p, C.c_int]
+                                  P(C.c_longlong), C.c_void_p, C.c_void_p, C.c_size_t,
+                                  C.c_void_p, C.c_int]
     lib.cs_clip_count.restype = C.c_int
     IP = P(C.c_int)
     lib.cs_dedisp_tables.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,

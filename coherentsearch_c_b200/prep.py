@@ -70,7 +70,11 @@ class PrepSearch:
         # the raw block may still be in flight on the caller's stream
         self.stream.wait_stream(torch.cuda.current_stream(self.dev))
         if self.clip_sigma > 0:
-            n = self.dd.clip_count(d_raw, nspec, self.clip_sigma, self.stream.cuda_stream)
+            need = self.dd.clip_scratch_bytes(nspec)
+            if getattr(self, "_clip_scratch", None) is None or self._clip_scratch.numel() < need:
+                self._clip_scratch = torch.empty(need, dtype=torch.uint8, device=self.dev)
+            n = self.dd.clip_count(d_raw, nspec, self.clip_sigma, self.stream.cuda_stream,
+                                   self._clip_scratch.data_ptr(), self._clip_scratch.numel())
             if n:
                 raise RuntimeError(
                     f"prepsubband's -clip {self.clip_sigma:g} would replace {n} spectra of this "

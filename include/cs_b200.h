@@ -154,9 +154,14 @@ void cs_ducy_free(CsDucy *d);
  * for each such spectrum.  The device front end runs without clipping; its
  * output equals the clipped run's exactly when *nclipped is 0 (counted over
  * every full block, also ones a run with a shorter numout never reads).
- * Returns 0 or -1. */
+ * d_scratch: device memory of cs_clip_scratch_bytes(nspec, L) bytes, 256-byte
+ * aligned, kept by the caller across calls; NULL makes the call allocate and
+ * free its own, which synchronises the device and can take far longer than
+ * the work.  Returns 0 or -1. */
+size_t cs_clip_scratch_bytes(long long nspec, int L);
 int cs_clip_count(const uint8_t *d_raw, long long nspec, int nchan, int L, float clip_sigma,
-                  long long *nclipped, uint8_t *d_flags, void *stream, int device);
+                  long long *nclipped, uint8_t *d_flags, void *d_scratch, size_t scratch_bytes,
+                  void *stream, int device);
 
 /* ---- SIGPROC filterbank header (in libcoherent_search.so) --------------
  * The header read_filterbank_header parses (third_party/presto/

@@ -60,6 +60,12 @@ def test_clip_count_matches_reference(gpu_ready, geom, nblocks):
             got = dd.clip_count(d.data_ptr(), data.shape[0], 6.0)
             torch.cuda.synchronize()
             assert got == want, (geom, got, want)
+            # with caller-kept scratch, twice (nothing carries over between calls)
+            scr = torch.empty(dd.clip_scratch_bytes(data.shape[0]), dtype=torch.uint8,
+                              device="cuda")
+            for _ in range(2):
+                assert dd.clip_count(d.data_ptr(), data.shape[0], 6.0, None, scr.data_ptr(),
+                                     scr.numel()) == want
         # a lower threshold clips more, in both
         data = _rfi(raw, L)
         _, want = _ref(data, t, 3.0)
