@@ -57,6 +57,21 @@ class Batch:
             raise RuntimeError(f"batch request {rid} failed (see stderr)")
         return out, q.value, r.value
 
+    def warm(self, N: int, dt: float, opts: Options | None = None) -> None:
+        """Load every slot for a length-N search with `opts` (no spectrum is
+        read), so that requests up to that size find their buffers grown."""
+        opts = opts or Options()
+        ft = nt.FFTFile()
+        ft.amps = None
+        ft.namps = N // 2
+        ft.N = N
+        ft.T = N * dt
+        ft.df = 1.0 / ft.T
+        p = opts.params(self.host)
+        if self.gpu.cs_gpu_batch_warm(self.h, C.byref(ft), C.byref(p), opts.lofreq, opts.hifreq,
+                                      opts.lobin, opts.blocksize) != 0:
+            raise RuntimeError("cs_gpu_batch_warm failed (see stderr)")
+
     def pending(self) -> int:
         return int(self.gpu.cs_gpu_batch_pending(self.h))
 

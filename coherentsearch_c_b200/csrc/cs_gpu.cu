@@ -1567,7 +1567,10 @@ struct BatchReq {
     CandidateList out;
     int status;                      /* 0 ok, -1 error */
     bool done;
-    std::chrono::steady_clock::time_point t_submit, t_start, t_end;
+    bool rekeyed;                    /* the slot's tables were rebuilt for it */
+    int only_slot = -1;              /* >= 0: only this slot takes it */
+    bool load_only = false;          /* build tables and buffers, no search */
+    std::chrono::steady_clock::time_point t_submit, t_start, t_admit, t_loaded, t_end;
 };
 
 /* What a slot's session was last loaded for. */
@@ -1597,6 +1600,7 @@ struct CsBatch {
     std::unordered_map<long long, BatchReq *> reqs;
     long long next_id = 0;
     bool stop = false;
+    bool trace = false;              /* CS_B200_BATCH_TRACE: phase times per request */
 };
 
 /* Geometry of a request, as search_file derives it (src/search.c:1247-1262). */
@@ -1688,7 +1692,9 @@ static void batch_run_one(CsBatch *B, int k, BatchReq *r)
         slot.S = S;
         slot.keyed = false;
     }
+    r->rekeyed = false;
     if (!slot.keyed || memcmp(&key, &slot.key, sizeof(key)) != 0) {
+        r->rekeyed = true;
         DirectPlanSet plans;
         memset(&plans, 0, sizeof(plans));
         long long *cstarts = NULL, nchunks = 0;
@@ -1704,7 +1710,12 @@ static void batch_run_one(CsBatch *B, int k, BatchReq *r)
         slot.key = key;
         slot.keyed = true;
     }
+    if (r->load_only) {
+        r->status = 0;
+        return;
+    }
     S->p = &r->p;
+    r->t_loaded = std::chrono::steady_clock::now();
     if (S->namps > 0 &&
         cudaMemcpyAsync(S->d_amps, r->ft.amps, (size_t)S->namps * sizeof(float2),
                         cudaMemcpyHostToDevice, S->st) != cudaSuccess) {
@@ -1732,16 +1743,23 @@ static void batch_worker(CsBatch *B, int k)
     select_device(B->device);
     std::unique_lock<std::mutex> lk(B->mu);
     for (;;) {
-        B->cv_work.wait(lk, [&] { return B->stop || !B->queue.empty(); });
-        if (B->stop && B->queue.empty()) break;
-        BatchReq *r = B->queue.front();
-        B->queue.pop_front();
+        auto mine = [&] {
+            auto it = B->queue.begin();
+            while (it != B->queue.end() && (*it)->only_slot >= 0 && (*it)->only_slot != k) ++it;
+            return it;
+        };
+        B->cv_work.wait(lk, [&] { return B->stop || mine() != B->queue.end(); });
+        const auto it = mine();
+        if (it == B->queue.end()) break;             /* stopping, nothing left for this slot */
+        BatchReq *r = *it;
+        B->queue.erase(it);
         double r_lo, lodr;
         long long total;
         int Nprof;
         const size_t need = batch_geometry(r, &r_lo, &lodr, &total, &Nprof)
                                 ? batch_footprint(r, total, Nprof) : 0;
-        r->t_start = std::chrono::steady_clock::now();
+        r->t_start = r->t_admit = r->t_loaded = std::chrono::steady_clock::now();
+        r->rekeyed = false;
         if (!batch_admit(B, k, need, lk)) {
             fprintf(stderr, "Error: batch request %lld needs about %zu device bytes, more than "
                             "the budget of %zu\n", r->id, need, B->budget);
@@ -1752,6 +1770,7 @@ static void batch_worker(CsBatch *B, int k)
             /* reserve the room while the slot grows into it */
             B->slots[k].bytes = std::max(B->slots[k].bytes, need);
             lk.unlock();
+            r->t_admit = r->t_loaded = std::chrono::steady_clock::now();
             batch_run_one(B, k, r);
             lk.lock();
             BatchSlot &slot = B->slots[k];
@@ -1759,6 +1778,13 @@ static void batch_worker(CsBatch *B, int k)
             slot.bytes = slot.S ? session_bytes(slot.S) : 0;
         }
         r->t_end = std::chrono::steady_clock::now();
+        if (B->trace) {
+            using ms = std::chrono::duration<double, std::milli>;
+            fprintf(stderr, "batch trace: id %lld slot %d N %lld nharms %d rekeyed %d "
+                            "admit %.3f load %.3f search %.3f ms\n", r->id, k, (long long)r->ft.N,
+                    r->p.nharms, (int)r->rekeyed, ms(r->t_admit - r->t_start).count(),
+                    ms(r->t_loaded - r->t_admit).count(), ms(r->t_end - r->t_loaded).count());
+        }
         r->done = true;
         B->cv_done.notify_all();
         B->cv_mem.notify_all();
@@ -1779,6 +1805,7 @@ CS_EXPORT CsBatch *cs_gpu_batch_create(int device, int nslots, size_t mem_budget
     CsBatch *B = new CsBatch();
     B->device = device;
     B->budget = mem_budget;
+    B->trace = getenv("CS_B200_BATCH_TRACE") != nullptr;
     B->slots.resize(nslots);
     for (int k = 0; k < nslots; k++) B->workers.emplace_back(batch_worker, B, k);
     return B;
@@ -1829,6 +1856,46 @@ CS_EXPORT int cs_gpu_batch_wait(CsBatch *B, long long id, CandidateList *out, do
     if (run_ms) *run_ms = ms(r->t_end - r->t_start).count();
     delete r;
     return status;
+}
+
+CS_EXPORT int cs_gpu_batch_warm(CsBatch *B, const FFTFile *ft, const SearchParams *p,
+                                double lofreq, double hifreq, int lobin, int blocksize)
+{
+    if (!B || !ft || !p) return -1;
+    std::vector<BatchReq *> mine;
+    {
+        std::lock_guard<std::mutex> g(B->mu);
+        for (int k = 0; k < (int)B->slots.size(); k++) {
+            BatchReq *r = new BatchReq();
+            r->ft = *ft;
+            r->ft.amps = NULL;                       /* nothing is uploaded */
+            r->p = *p;
+            r->lofreq = lofreq;
+            r->hifreq = hifreq;
+            r->lobin = lobin;
+            r->blocksize = blocksize;
+            r->threshold = p->threshold;
+            r->status = -1;
+            r->done = false;
+            r->only_slot = k;
+            r->load_only = true;
+            candlist_init(&r->out);
+            r->t_submit = std::chrono::steady_clock::now();
+            r->id = B->next_id++;
+            B->queue.push_back(r);
+            mine.push_back(r);
+        }
+    }
+    B->cv_work.notify_all();
+    int rc = 0;
+    std::unique_lock<std::mutex> lk(B->mu);
+    for (BatchReq *r : mine) {
+        B->cv_done.wait(lk, [&] { return r->done; });
+        if (r->status != 0) rc = -1;
+        candlist_free(&r->out);
+        delete r;
+    }
+    return rc;
 }
 
 CS_EXPORT int cs_gpu_batch_pending(CsBatch *B)

@@ -50,6 +50,7 @@ class SearchServer:
         # one waiter per in-flight request, so a result is seen when it lands
         self.pool = cf.ThreadPoolExecutor(max_workers=64)
         self.lock = threading.Lock()
+        self.stats: list[tuple[float, float]] = []   # (ms queued for a slot, ms on the slot)
 
     def submit(self, amps, N: int, dt: float, opts: Options | None = None,
                arrival: float | None = None) -> cf.Future:
@@ -58,10 +59,20 @@ class SearchServer:
             rid = self.batch.submit(amps, N, dt, opts)
 
         def finish():
-            cands, _, _ = self.batch.wait(rid)
+            cands, queued, run = self.batch.wait(rid)
+            with self.lock:
+                self.stats.append((queued, run))
             return cands, 1e3 * (time.perf_counter() - t0)
 
         return self.pool.submit(finish)
+
+    def warm(self, N: int, dt: float, opts: Options | None = None) -> None:
+        """Grow every slot's device buffers to the largest request expected
+        (length N with `opts`; nharms 60 needs the largest tables) before
+        traffic arrives.  A slot that grows while serving frees and allocates
+        device memory, and cudaFree waits for the whole device, so the other
+        slots' requests stall behind it."""
+        self.batch.warm(N, dt, opts or Options())
 
     def close(self) -> None:
         self.pool.shutdown(wait=True)

@@ -103,6 +103,15 @@ long long cs_gpu_batch_submit(CsBatch *b, const FFTFile *ft, const SearchParams 
 int cs_gpu_batch_wait(CsBatch *b, long long id, CandidateList *out, double *queued_ms,
                       double *run_ms);
 
+/* Load every slot for the geometry of a request (ft->N, ft->namps, ft->T and
+ * the band; ft->amps is not read) and return once all slots have built their
+ * tables and grown their device buffers to it.  A server calls it before
+ * traffic with its largest request: a slot that grows while serving frees
+ * device memory, and cudaFree waits for the whole device, other slots'
+ * searches included.  Returns 0, or -1 if a slot failed. */
+int cs_gpu_batch_warm(CsBatch *b, const FFTFile *ft, const SearchParams *p, double lofreq,
+                      double hifreq, int lobin, int blocksize);
+
 /* Requests submitted and not yet waited for. */
 int cs_gpu_batch_pending(CsBatch *b);
 

@@ -80,3 +80,18 @@ def test_batch_rejects_request_beyond_budget(gpu_ready, cases):
         rid = b.submit(amps, 1 << nlog, DT, opts_for(nh))
         with pytest.raises(RuntimeError):
             b.wait(rid)
+
+
+def test_batch_warm_then_serve(gpu_ready, cases):
+    """Slots loaded ahead for the largest request (nharms 60, a longer
+    spectrum than any case) serve every case with unchanged results; the
+    load-only requests leave nothing pending."""
+    with Batch(nslots=3) as b:
+        b.warm(1 << 18, DT, opts_for(60))
+        assert b.pending() == 0
+        ids = [b.submit(amps, 1 << nlog, DT, opts_for(nh)) for nlog, nh, amps, _ in cases]
+        for rid, (_, _, _, ref) in zip(ids, cases):
+            same(b.wait(rid)[0], ref)
+        b.warm(1 << 15, DT, opts_for(16))           # smaller: reuses the buffers
+        rid = b.submit(cases[0][2], 1 << cases[0][0], DT, opts_for(cases[0][1]))
+        same(b.wait(rid)[0], cases[0][3])
