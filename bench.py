@@ -1066,7 +1066,7 @@ def run_series(args):
                    "parallelism": "replicas1"},
         "e2e": {"value": total / (statistics.mean(e2e) * 1e-3), "unit": UNIT,
                 "h2d_bytes_per_step": int(x.nbytes), "d2h_bytes_per_step": int(out.nbytes)},
-        "gpu_launches": 15 * args.steps,
+        "gpu_launches": 16 * args.steps,     # 4 spectrum, 2 search, 10 collapse (cuFFT, CUB not counted)
         "roofline": {"bound": "tensor", "achieved": dft, "peak": tc_peak, "unit": "TFLOP/s",
                      "frac": dft / tc_peak, "traffic": None,
                      "kernel": "search_ws60" if ses.info().kernel == 1 else "cs_search_kernel",
