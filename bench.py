@@ -667,13 +667,13 @@ def run_prep(args):
     value = world * trials / (ms * 1e-3)
     hbm_peak, tc_peak, peak_kind = load_peaks()
     kms = statistics.mean(search_ms)
-    # the default 6-sigma clip check, timed on its own (it runs inside each step)
+    # the default 6-sigma clip decisions and channel levels, timed on their
+    # own (they run inside each step, before the dedispersion)
     torch.cuda.synchronize()
     c0 = time.perf_counter()
-    scr = getattr(ps, "_clip_scratch", None)
-    ps.dd.clip_count(raw.data_ptr(), spec.nspec, ps.clip_sigma or 6.0, stream.cuda_stream,
-                     scr.data_ptr() if scr is not None else None,
-                     scr.numel() if scr is not None else 0)
+    ps.dd.clip_levels(raw.data_ptr(), spec.nspec, ps._clip_flags.data_ptr(),
+                      ps._clip_levels.data_ptr(), ps.clip_sigma, stream.cuda_stream,
+                      ps._clip_scratch.data_ptr(), ps._clip_scratch.numel())
     clip_ms = 1e3 * (time.perf_counter() - c0)
     dft_tflops = trials * DFT_FLOP_PER_TRIAL / (kms * 1e-3) / 1e12
     line = {
@@ -689,7 +689,9 @@ def run_prep(args):
                        output_per_dm=ps.nout,
                        l2="inputs larger than L2 (raw input and dedispersed output > 126 MB)",
                        parallelism=f"replicas{world}"),
-        "gpu_launches": (2 + 6 * t.ndm) * args.steps,
+        # clip decisions and levels 6, dedispersion 2; per DM spectrum 4, search 2,
+        # collapse 10 (cuFFT, CUB and PyTorch's fills not counted)
+        "gpu_launches": (8 + 16 * t.ndm) * args.steps,
         "roofline": {"bound": "tensor", "achieved": dft_tflops, "peak": tc_peak,
                      "unit": "TFLOP/s", "frac": dft_tflops / tc_peak, "traffic": None,
                      "kernel": "search_ws60", "kernel_ms_per_dm": kms / t.ndm,
@@ -698,7 +700,8 @@ def run_prep(args):
                                     f"x {t.ndm} DMs"},
         "stages_ms": {"dedisp": statistics.mean(dd_ms), "search_kernels": kms,
                       "rest": ms - statistics.mean(dd_ms) - kms,
-                      "clip_check": clip_ms, "steps": [round(x, 2) for x in times]},
+                      "clip_levels": clip_ms, "steps": [round(x, 2) for x in times]},
+        "spectra_clipped": ps.nclipped,
         "clocks": clk.summary(),
         "candidates": ncand,
     }

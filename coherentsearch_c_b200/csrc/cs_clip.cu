@@ -20,13 +20,20 @@
  *                    |zdm[t] - running_mean| > clip_sigma * running_sigma
  *                    (the difference in float, the test in double).
  *
- * The replacement values (channel running levels) are not produced: the
- * device front end implements prepsubband without clipping, and a run with
- * -clip is the same run exactly when this count is zero.  The arithmetic is
- * the reference's without fast-math rewriting (this file is built with
- * -fmad=false); the reference's -Ofast build can move its sigma in the last
- * bits, which only matters for a spectrum within that distance of the
- * trigger.
+ *   replacement      a replaced spectrum takes the block's channel levels:
+ *                    per channel the sum over the block's good spectra (an
+ *                    integer, exact) over their number, in double, then the
+ *                    running level, a float: the first block's value, then
+ *                    0.9 * old + 0.1 * new in double (clipping.c:118-160);
+ *                    a block without good spectra keeps the old level.
+ *
+ * cs_clip_count gives the number of replaced spectra (and optionally the
+ * flags); cs_clip_levels adds the levels, which the clipped dedispersion
+ * (cs_dedisp_run_device_clipped) substitutes.  The arithmetic is the
+ * reference's as its build compiles it (-ffp-contract=off, src/Makefile:43):
+ * this file is built with -fmad=false.  Its -Ofast may still rewrite a
+ * division by the good count as a reciprocal product; that changes the
+ * double value by an ulp at most, below what the float level keeps.
  */
 #include <cuda_runtime.h>
 
@@ -92,6 +99,7 @@ struct AvgVar {
 
 struct BlockStats {
     int ngood;
+    float lo, hi;            /* good samples lie strictly between */
     double mean, sigma;      /* of the good samples */
 };
 
@@ -134,6 +142,8 @@ __global__ void __launch_bounds__(NT) block_kernel(const int *zdm, int L, int P2
         if (v > lo && v < hi) good.push(v);
     }
     BlockStats s;
+    s.lo = lo;
+    s.hi = hi;
     s.ngood = (int)good.n;
     s.mean = good.mean;
     s.sigma = good.n ? sqrt(good.var()) : 0.0;
@@ -178,6 +188,39 @@ __global__ void decide_kernel(const int *zdm, long long n, int L, const float *r
     if (clip) atomicAdd(count, 1ull);
 }
 
+/* per (block, channel column): the sum of the column over the block's good
+ * spectra, stored as a float (an integer below 2^24: exact) */
+__global__ void chan_sum_kernel(const uint8_t *raw, int L, int nchan, const int *zdm,
+                                const BlockStats *st, float *sums)
+{
+    const long long b = blockIdx.x;
+    const int c = blockIdx.y * blockDim.x + threadIdx.x;
+    if (c >= nchan) return;
+    const float lo = st[b].lo, hi = st[b].hi;
+    const uint8_t *col = raw + b * L * (long long)nchan + c;
+    unsigned s = 0;
+    for (int i = 0; i < L; i++) {
+        const float v = (float)zdm[b * L + i];
+        if (v > lo && v < hi) s += __ldg(col + (long long)i * nchan);
+    }
+    sums[b * nchan + c] = (float)s;
+}
+
+/* running channel levels from block to block, in place over the sums (one
+ * thread per channel column) */
+__global__ void levels_kernel(const BlockStats *st, long long nblocks, int nchan, float *lv)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nchan) return;
+    float run = 0.0f;
+    for (long long b = 0; b < nblocks; b++) {
+        const int ng = st[b].ngood;
+        const double cur = ng >= 1 ? (double)lv[b * nchan + c] / (double)ng : (double)run;
+        run = b ? (float)(0.9 * (double)run + 0.1 * cur) : (float)cur;
+        lv[b * nchan + c] = run;
+    }
+}
+
 }  // namespace ck
 
 /* scratch layout: zero-DM sums, block statistics, running values, count */
@@ -201,9 +244,9 @@ CS_EXPORT size_t cs_clip_scratch_bytes(long long nspec, int L)
     return clip_layout(nspec, L, off);
 }
 
-CS_EXPORT int cs_clip_count(const uint8_t *d_raw, long long nspec, int nchan, int L,
-                            float clip_sigma, long long *nclipped, uint8_t *d_flags,
-                            void *d_scratch, size_t scratch_bytes, void *stream, int device)
+static int clip_run(const uint8_t *d_raw, long long nspec, int nchan, int L, float clip_sigma,
+                    long long *nclipped, uint8_t *d_flags, float *d_levels, void *d_scratch,
+                    size_t scratch_bytes, void *stream, int device, const char *who)
 {
     if (!nclipped || nchan < 1 || L < 1 || L > ck::MAX_L || nspec < 0) return -1;
     *nclipped = 0;
@@ -224,8 +267,7 @@ CS_EXPORT int cs_clip_count(const uint8_t *d_raw, long long nspec, int nchan, in
     if (own) {
         e = cudaMalloc((void **)&base, need);
     } else if (scratch_bytes < need || ((uintptr_t)d_scratch & 255)) {
-        fprintf(stderr, "Error: cs_clip_count: scratch of %zu bytes (256-byte aligned) needed\n",
-                need);
+        fprintf(stderr, "Error: %s: scratch of %zu bytes (256-byte aligned) needed\n", who, need);
         return -1;
     }
     int *zdm = (int *)(base + off[0]);
@@ -245,6 +287,12 @@ CS_EXPORT int cs_clip_count(const uint8_t *d_raw, long long nspec, int nchan, in
         ck::running_kernel<<<1, 1, 0, st>>>(bs, nblocks, clip_sigma, ravg, trig);
         ck::decide_kernel<<<(unsigned)((n + ck::NT - 1) / ck::NT), ck::NT, 0, st>>>(
             zdm, n, L, ravg, trig, cnt, d_flags);
+        if (d_levels) {
+            const dim3 g((unsigned)nblocks, (unsigned)((nchan + ck::NT - 1) / ck::NT));
+            ck::chan_sum_kernel<<<g, ck::NT, 0, st>>>(d_raw, L, nchan, zdm, bs, d_levels);
+            ck::levels_kernel<<<(nchan + ck::NT - 1) / ck::NT, ck::NT, 0, st>>>(bs, nblocks,
+                                                                              nchan, d_levels);
+        }
         e = cudaGetLastError();
     }
     if (e == cudaSuccess)
@@ -252,9 +300,30 @@ CS_EXPORT int cs_clip_count(const uint8_t *d_raw, long long nspec, int nchan, in
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (own) cudaFree(base);
     if (e != cudaSuccess) {
-        fprintf(stderr, "Error: cs_clip_count: %s\n", cudaGetErrorString(e));
+        fprintf(stderr, "Error: %s: %s\n", who, cudaGetErrorString(e));
         return -1;
     }
     *nclipped = (long long)hcnt;
     return 0;
+}
+
+CS_EXPORT int cs_clip_count(const uint8_t *d_raw, long long nspec, int nchan, int L,
+                            float clip_sigma, long long *nclipped, uint8_t *d_flags,
+                            void *d_scratch, size_t scratch_bytes, void *stream, int device)
+{
+    return clip_run(d_raw, nspec, nchan, L, clip_sigma, nclipped, d_flags, nullptr, d_scratch,
+                    scratch_bytes, stream, device, "cs_clip_count");
+}
+
+CS_EXPORT int cs_clip_levels(const uint8_t *d_raw, long long nspec, int nchan, int L,
+                             float clip_sigma, long long *nclipped, uint8_t *d_flags,
+                             float *d_levels, void *d_scratch, size_t scratch_bytes, void *stream,
+                             int device)
+{
+    if (!d_flags || !d_levels) {
+        if (nclipped) *nclipped = 0;
+        return -1;
+    }
+    return clip_run(d_raw, nspec, nchan, L, clip_sigma, nclipped, d_flags, d_levels, d_scratch,
+                    scratch_bytes, stream, device, "cs_clip_levels");
 }

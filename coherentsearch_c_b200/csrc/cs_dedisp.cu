@@ -121,16 +121,22 @@ struct SubArgs {
     long long sfill;          /* samples written per subband */
     uint16_t *sub;
     long long sstride;
+    /* clipped runs (dd_subband_clip) */
+    const uint8_t *flags;     /* [nflags] 1: spectrum replaced */
+    long long nflags;
+    const float *levels;      /* [nspec / L][nchan] channel levels, SIGPROC order */
+    int L;
+    int flag_off;             /* shared byte offset of the staged row flags */
+    float *subf;              /* S as float */
 };
 
-__global__ void __launch_bounds__(SB_THREADS) dd_subband_u8(const SubArgs a)
+/* Stage the CTA's raw rows [T0, T0 + SB_TT + halo) of its slab's channel
+ * columns in shared memory (padded rows), and the per-channel offsets of the
+ * delayed samples (coff).  Ends with a barrier. */
+static __device__ __forceinline__ void sb_stage(const SubArgs &a, unsigned char *sm, int s0,
+                                                int sc, long long T0)
 {
-    extern __shared__ __align__(16) unsigned char sm[];
-    const int s0 = blockIdx.x * a.slab;                   /* first subband */
-    const int nslab = min(a.slab, a.nsub - s0);
-    const int sc = nslab * a.cps;                         /* channels staged */
     const int c0 = s0 * a.cps;                            /* first channel */
-    const long long T0 = (long long)blockIdx.y * SB_TT;
     const int rows = SB_TT + a.halo;
     /* raw columns [col0, col0 + sc) hold channels c0 + sc - 1 .. c0 */
     const int col0 = a.nchan - c0 - sc;
@@ -164,6 +170,17 @@ __global__ void __launch_bounds__(SB_THREADS) dd_subband_u8(const SubArgs a)
         }
     }
     __syncthreads();
+}
+
+__global__ void __launch_bounds__(SB_THREADS) dd_subband_u8(const SubArgs a)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int s0 = blockIdx.x * a.slab;                   /* first subband */
+    const int nslab = min(a.slab, a.nsub - s0);
+    const int sc = nslab * a.cps;                         /* channels staged */
+    const long long T0 = (long long)blockIdx.y * SB_TT;
+    sb_stage(a, sm, s0, sc, T0);
+    const int *coff = reinterpret_cast<const int *>(sm + a.table_off);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nwarps = blockDim.x >> 5;
@@ -182,6 +199,54 @@ __global__ void __launch_bounds__(SB_THREADS) dd_subband_u8(const SubArgs a)
             for (int k = 0; k < a.cps; k++) acc += base[co[k]];
         }
         a.sub[(long long)(s0 + sl) * a.sstride + T] = (uint16_t)acc;
+    }
+}
+
+/* The subband stage of a clipped run: spectra flagged by the clip decisions
+ * take their block's channel levels (floats), so the sums are evaluated as
+ * the reference does (dispersion.c:245-264): in FP32, from 0.0f, adding the
+ * channels in ascending frequency.  S is float here. */
+__global__ void __launch_bounds__(SB_THREADS) dd_subband_clip(const SubArgs a)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int s0 = blockIdx.x * a.slab;
+    const int nslab = min(a.slab, a.nsub - s0);
+    const int sc = nslab * a.cps;
+    const long long T0 = (long long)blockIdx.y * SB_TT;
+    const int rows = SB_TT + a.halo;
+    unsigned char *rflag = sm + a.flag_off;              /* clip flag of each staged row */
+    for (int r = threadIdx.x; r < rows; r += blockDim.x)
+        rflag[r] = T0 + r < a.nflags ? a.flags[T0 + r] : 0;
+    sb_stage(a, sm, s0, sc, T0);
+    const int *coff = reinterpret_cast<const int *>(sm + a.table_off);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nwarps = blockDim.x >> 5;
+    const int ngroups = SB_TT / 32;
+    for (int item = warp; item < nslab * ngroups; item += nwarps) {
+        const int sl = item / ngroups, g = item - sl * ngroups;
+        const int t = g * 32 + lane;
+        const long long T = T0 + t;
+        if (T >= a.sfill) continue;
+        float acc = 0.0f;
+        if (T < a.nvalid) {
+            const unsigned char *base = sm + (size_t)t * a.rowstride;
+            const int cfirst = (s0 + sl) * a.cps;
+            const int *co = coff + sl * a.cps;
+            for (int k = 0; k < a.cps; k++) {
+                const int c = cfirst + k;
+                const int r = t + __ldg(a.idisp + c);
+                float x;
+                if (rflag[r]) {
+                    const long long u = T0 + r;
+                    x = __ldg(a.levels + (u / a.L) * a.nchan + (a.nchan - 1 - c));
+                } else {
+                    x = (float)base[co[k]];
+                }
+                acc = __fadd_rn(acc, x);
+            }
+        }
+        a.subf[(long long)(s0 + sl) * a.sstride + T] = acc;
     }
 }
 
@@ -317,6 +382,25 @@ __global__ void __launch_bounds__(256) dd_dms_u16_direct(const DmArgs a)
     a.out[(long long)d * a.ostride + T] = (float)acc;
 }
 
+/* The DM stage of a clipped run: S is float, summed as float_dedisp does
+ * (dispersion.c:322-365): from -approx_mean = -0.0f, adding the subbands in
+ * ascending order in FP32.  One thread per (DM, sample); the DM index varies
+ * fastest over the grid, so CTAs running together read the same stretch of
+ * S and share it through L2. */
+__global__ void __launch_bounds__(256) dd_dms_f32(const float *subf, long long sstride, int nsub,
+                                                  int ndm, const int *offs, long long nout,
+                                                  float *out, long long ostride)
+{
+    const int d = (int)(blockIdx.x % (unsigned)ndm);
+    const long long T = (long long)(blockIdx.x / (unsigned)ndm) * blockDim.x + threadIdx.x;
+    if (T >= nout) return;
+    const int *off = offs + (size_t)d * nsub;
+    float acc = -0.0f;
+    for (int s = 0; s < nsub; s++)
+        acc = __fadd_rn(acc, __ldg(subf + (long long)s * sstride + T + __ldg(off + s)));
+    out[(long long)d * ostride + T] = acc;
+}
+
 }  // namespace dd
 
 /* ---------------------------------------------------------------- */
@@ -337,6 +421,7 @@ struct CsDedisp {
     int *d_code = nullptr, *d_nch = nullptr;
     long long *d_chunk = nullptr;
     uint16_t *d_sub = nullptr;
+    float *d_subf = nullptr;       /* S of clipped runs (allocated by the first one) */
     long long sstride = 0;
     uint8_t *d_raw = nullptr;      /* staging for the host-memory entry point */
     float *d_out = nullptr;
@@ -354,6 +439,7 @@ static void dd_release(CsDedisp *D)
     cudaFree(D->d_nch);
     cudaFree(D->d_chunk);
     cudaFree(D->d_sub);
+    cudaFree(D->d_subf);
     cudaFree(D->d_raw);
     cudaFree(D->d_out);
     if (D->st) cudaStreamDestroy(D->st);
@@ -443,9 +529,15 @@ static int sb_table_offset(const CsDedisp *D, int slab)
     return ((dd::SB_TT + D->halo) * sb_rowstride(D, slab) + 15) / 16 * 16;
 }
 
-static int sb_smem(const CsDedisp *D, int slab)
+static int sb_flag_offset(const CsDedisp *D, int slab)
 {
     return sb_table_offset(D, slab) + slab * D->cps * 4;
+}
+
+/* the clipped kernel also stages one flag byte per row */
+static int sb_smem(const CsDedisp *D, int slab, bool clip = false)
+{
+    return sb_flag_offset(D, slab) + (clip ? dd::SB_TT + D->halo : 0);
 }
 
 CS_EXPORT CsDedisp *cs_dedisp_create(int nchan, int nsub, int ndm, const int *idispdt,
@@ -603,6 +695,8 @@ CS_EXPORT CsDedisp *cs_dedisp_create(int nchan, int nsub, int ndm, const int *id
                                   (int)dm_smem));
     DDCK(cudaFuncSetAttribute(dd::dd_subband_u8, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               max_optin));
+    DDCK(cudaFuncSetAttribute(dd::dd_subband_clip, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              max_optin));
     /* a copy from pageable memory may return before its DMA lands; finish
      * them all before a run on any stream can read the tables */
     DDCK(cudaDeviceSynchronize());
@@ -611,8 +705,10 @@ CS_EXPORT CsDedisp *cs_dedisp_create(int nchan, int nsub, int ndm, const int *id
 }
 
 static cudaError_t dd_enqueue(CsDedisp *D, const uint8_t *d_raw, long long nspec, long long nout,
-                              float *d_out, long long ostride, cudaStream_t st)
+                              float *d_out, long long ostride, cudaStream_t st,
+                              const uint8_t *d_flags = nullptr, const float *d_levels = nullptr)
 {
+    const bool clip = d_flags != nullptr;
     if (nout <= 0) return cudaSuccess;
     /* subband stage over every sample the DM stage can read */
     const long long ntile_dm = (nout + dd::DM_TT - 1) / dd::DM_TT;
@@ -620,7 +716,7 @@ static cudaError_t dd_enqueue(CsDedisp *D, const uint8_t *d_raw, long long nspec
     int max_optin = 0;
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, D->device);
     int slab = std::max(1, std::min(D->nsub, 256 / std::max(1, D->cps)));
-    while (slab > 1 && sb_smem(D, slab) > std::min(max_optin, 100 * 1024)) slab /= 2;
+    while (slab > 1 && sb_smem(D, slab, clip) > std::min(max_optin, 100 * 1024)) slab /= 2;
     dd::SubArgs sa;
     sa.raw = d_raw;
     sa.nspec = nspec;
@@ -636,11 +732,28 @@ static cudaError_t dd_enqueue(CsDedisp *D, const uint8_t *d_raw, long long nspec
     sa.sfill = sfill;
     sa.sub = D->d_sub;
     sa.sstride = D->sstride;
+    sa.flags = d_flags;
+    sa.nflags = nspec / D->L * D->L;
+    sa.levels = d_levels;
+    sa.L = D->L;
+    sa.flag_off = sb_flag_offset(D, slab);
+    sa.subf = D->d_subf;
     dim3 gs((D->nsub + slab - 1) / slab, (unsigned)((sfill + dd::SB_TT - 1) / dd::SB_TT));
     cudaEventRecord(D->ev0, st);
-    dd::dd_subband_u8<<<gs, dd::SB_THREADS, sb_smem(D, slab), st>>>(sa);
+    if (clip)
+        dd::dd_subband_clip<<<gs, dd::SB_THREADS, sb_smem(D, slab, true), st>>>(sa);
+    else
+        dd::dd_subband_u8<<<gs, dd::SB_THREADS, sb_smem(D, slab), st>>>(sa);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    if (clip) {
+        const long long ntile = (nout + 255) / 256;
+        cudaEventRecord(D->ev1, st);
+        dd::dd_dms_f32<<<(unsigned)(ntile * D->ndm), 256, 0, st>>>(
+            D->d_subf, D->sstride, D->nsub, D->ndm, D->d_offs, nout, d_out, ostride);
+        cudaEventRecord(D->ev2, st);
+        return cudaGetLastError();
+    }
     dd::DmArgs da;
     da.sub = D->d_sub;
     da.sstride = D->sstride;
@@ -693,6 +806,45 @@ CS_EXPORT int cs_dedisp_run_device(CsDedisp *D, const uint8_t *d_raw, long long 
     cudaError_t e = dd_enqueue(D, d_raw, nspec, nout, d_out, out_stride, st);
     if (e != cudaSuccess) {
         fprintf(stderr, "Error: cs_dedisp_run: %s\n", cudaGetErrorString(e));
+        return -1;
+    }
+    if (nout_written) *nout_written = nout;
+    return 0;
+}
+
+CS_EXPORT int cs_dedisp_run_device_clipped(CsDedisp *D, const uint8_t *d_raw, long long nspec,
+                                           long long numout, const uint8_t *d_flags,
+                                           const float *d_levels, float *d_out,
+                                           long long out_stride, void *stream,
+                                           long long *nout_written)
+{
+    if (nout_written) *nout_written = 0;
+    if (!D || !d_raw || !d_out || !d_flags || !d_levels) return -1;
+    if (nspec > D->max_spectra) {
+        fprintf(stderr, "Error: cs_dedisp_run_device_clipped: %lld spectra exceed the plan's "
+                        "%lld\n", nspec, D->max_spectra);
+        return -1;
+    }
+    const long long nout = cs_dedisp_output_length(D, nspec, numout);
+    if (out_stride < nout || (out_stride & 3) || ((uintptr_t)d_out & 15)) {
+        fprintf(stderr, "Error: cs_dedisp_run_device_clipped: out_stride must be >= %lld and a "
+                        "multiple of 4, the output 16-byte aligned\n", nout);
+        return -1;
+    }
+    if ((unsigned long long)((nout + 255) / 256) * (unsigned long long)D->ndm >= (1ULL << 31)) {
+        fprintf(stderr, "Error: cs_dedisp_run_device_clipped: %lld points x %d DMs is too many "
+                        "for one launch\n", nout, D->ndm);
+        return -1;
+    }
+    if (cudaSetDevice(D->device) != cudaSuccess) return -1;
+    cudaError_t e = cudaSuccess;
+    if (!D->d_subf)
+        e = cudaMalloc((void **)&D->d_subf, sizeof(float) * (size_t)D->nsub * D->sstride);
+    cudaStream_t st = stream ? (cudaStream_t)stream : D->st;
+    if (e == cudaSuccess) e = dd_enqueue(D, d_raw, nspec, nout, d_out, out_stride, st, d_flags,
+                                         d_levels);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "Error: cs_dedisp_run_device_clipped: %s\n", cudaGetErrorString(e));
         return -1;
     }
     if (nout_written) *nout_written = nout;

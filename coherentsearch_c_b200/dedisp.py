@@ -105,6 +105,35 @@ class Dedisperser:
             raise RuntimeError("cs_dedisp_run_device failed (see stderr)")
         return got.value
 
+    def run_device_clipped(self, d_raw: int, nspec: int, d_flags: int, d_levels: int,
+                           d_out: int, out_stride: int, numout: int = -1,
+                           stream: int | None = None) -> int:
+        """cs_dedisp_run_device_clipped: the run prepsubband makes with -clip,
+        given clip_levels' flags and levels (device pointers); returns points
+        per DM.  The first clipped run allocates the plan's float subbands."""
+        got = C.c_longlong(0)
+        rc = self.lib.cs_dedisp_run_device_clipped(self.plan, d_raw, nspec, numout, d_flags,
+                                                   d_levels, d_out, out_stride, stream,
+                                                   C.byref(got))
+        if rc != 0:
+            raise RuntimeError("cs_dedisp_run_device_clipped failed (see stderr)")
+        return got.value
+
+    def clip_levels(self, d_raw: int, nspec: int, d_flags: int, d_levels: int,
+                    clip_sigma: float = 6.0, stream: int | None = None,
+                    scratch: int | None = None, scratch_bytes: int = 0) -> int:
+        """cs_clip_levels: the count of replaced spectra, their flags
+        (nspec // L * L bytes at d_flags) and clip_times' channel levels after
+        each block ([nspec // L][nchan] floats at d_levels, SIGPROC channel
+        order)."""
+        n = C.c_longlong(0)
+        rc = self.lib.cs_clip_levels(d_raw, nspec, self.t.nchan, self.t.spectra_per_subint,
+                                     float(clip_sigma), C.byref(n), d_flags, d_levels, scratch,
+                                     scratch_bytes, stream, self.device)
+        if rc != 0:
+            raise RuntimeError("cs_clip_levels failed (see stderr)")
+        return n.value
+
     def clip_scratch_bytes(self, nspec: int) -> int:
         return int(self.lib.cs_clip_scratch_bytes(nspec, self.t.spectra_per_subint))
 

@@ -197,6 +197,10 @@ def declare_gpu_api(lib: C.CDLL) -> C.CDLL:
                                   P(C.c_longlong), C.c_void_p, C.c_void_p, C.c_size_t,
                                   C.c_void_p, C.c_int]
     lib.cs_clip_count.restype = C.c_int
+    lib.cs_clip_levels.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_float,
+                                   P(C.c_longlong), C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_size_t, C.c_void_p, C.c_int]
+    lib.cs_clip_levels.restype = C.c_int
     IP = P(C.c_int)
     lib.cs_dedisp_tables.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                      C.c_double, C.c_double, C.c_double, C.c_int, IP, IP, IP,
@@ -211,6 +215,11 @@ def declare_gpu_api(lib: C.CDLL) -> C.CDLL:
                                          C.c_void_p, C.c_longlong, C.c_void_p,
                                          P(C.c_longlong)]
     lib.cs_dedisp_run_device.restype = C.c_int
+    lib.cs_dedisp_run_device_clipped.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong,
+                                                 C.c_longlong, C.c_void_p, C.c_void_p,
+                                                 C.c_void_p, C.c_longlong, C.c_void_p,
+                                                 P(C.c_longlong)]
+    lib.cs_dedisp_run_device_clipped.restype = C.c_int
     lib.cs_dedisp_run.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_longlong,
                                   C.c_void_p, C.c_longlong, P(C.c_longlong)]
     lib.cs_dedisp_run.restype = C.c_int

@@ -2,7 +2,8 @@
 dedispersion -> for every DM, the series padded to `numout` points ->
 realfft + rednoise -> coherent search, as the reference's
 prep_coherent_search runs it (src/prep_dedisp.c:484-522, 744-790;
-src/prep_search.c) without clipping, masking, downsampling or barycentring.
+src/prep_search.c), with prepsubband's time-domain clipping (-clip, 6 sigma
+by default) and without masking, downsampling or barycentring.
 
 Every stage stays on the device: the dedispersed series are written into a
 [ndm][numout] buffer, padded there, turned into spectra in a session's device
@@ -58,9 +59,9 @@ class PrepSearch:
         self.sessions = [Session(self.N, dt, self.opts, device=device) for _ in range(4)]
         self.ses = self.sessions[0]
         self.pad_value = None
-        # prepsubband clips at 6 sigma unless told -noclip (0 here): the device
-        # path has no clipping, so it checks that clipping would change nothing
+        # prepsubband clips at 6 sigma unless told -noclip (0 here)
         self.clip_sigma = float(clip_sigma)
+        self.nclipped = 0                    # spectra the last dedisperse replaced
         self.search_ms: list[float] = []     # search kernel time of each DM, last pass
 
     def dedisperse(self, d_raw: int, nspec: int) -> None:
@@ -69,19 +70,26 @@ class PrepSearch:
         torch = self.torch
         # the raw block may still be in flight on the caller's stream
         self.stream.wait_stream(torch.cuda.current_stream(self.dev))
+        self.nclipped = 0
         if self.clip_sigma > 0:
-            need = self.dd.clip_scratch_bytes(nspec)
-            if getattr(self, "_clip_scratch", None) is None or self._clip_scratch.numel() < need:
-                self._clip_scratch = torch.empty(need, dtype=torch.uint8, device=self.dev)
-            n = self.dd.clip_count(d_raw, nspec, self.clip_sigma, self.stream.cuda_stream,
-                                   self._clip_scratch.data_ptr(), self._clip_scratch.numel())
-            if n:
-                raise RuntimeError(
-                    f"prepsubband's -clip {self.clip_sigma:g} would replace {n} spectra of this "
-                    "filterbank; the device front end has no clipping (pass clip_sigma=0 for "
-                    "the unclipped series, prepsubband's -noclip)")
-        n = self.dd.run_device(d_raw, nspec, self.out.data_ptr(), self.stride, self.N,
-                               self.stream.cuda_stream)
+            L = self.t.spectra_per_subint
+            nblk = nspec // L
+            # kept across calls: allocating here would synchronise the device
+            self._clip_scratch = self._keep("_clip_scratch", self.dd.clip_scratch_bytes(nspec),
+                                            torch.uint8)
+            self._clip_flags = self._keep("_clip_flags", nblk * L, torch.uint8)
+            self._clip_levels = self._keep("_clip_levels", nblk * self.t.nchan, torch.float32)
+            self.nclipped = self.dd.clip_levels(
+                d_raw, nspec, self._clip_flags.data_ptr(), self._clip_levels.data_ptr(),
+                self.clip_sigma, self.stream.cuda_stream, self._clip_scratch.data_ptr(),
+                self._clip_scratch.numel())
+        if self.nclipped:
+            n = self.dd.run_device_clipped(d_raw, nspec, self._clip_flags.data_ptr(),
+                                           self._clip_levels.data_ptr(), self.out.data_ptr(),
+                                           self.stride, self.N, self.stream.cuda_stream)
+        else:
+            n = self.dd.run_device(d_raw, nspec, self.out.data_ptr(), self.stride, self.N,
+                                   self.stream.cuda_stream)
         if n != self.nout:
             raise RuntimeError(f"dedispersion wrote {n} samples per DM, expected {self.nout}")
         if self.nout < self.N:
@@ -90,6 +98,13 @@ class PrepSearch:
             self.pad_value = float(np.float32(running_mean(head.numpy())))
             with torch.cuda.stream(self.stream):
                 self.out[:, self.nout:self.N].fill_(self.pad_value)
+
+    def _keep(self, name: str, n: int, dtype):
+        """A device buffer of at least n elements, grown only when too small."""
+        buf = getattr(self, name, None)
+        if buf is None or buf.numel() < n:
+            buf = self.torch.empty(max(1, n), dtype=dtype, device=self.dev)
+        return buf
 
     def _spectrum(self, d: int, ses: Session) -> None:
         self.spec.run_device(self.out[d].data_ptr(), ses.device_amps_ptr(),

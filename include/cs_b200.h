@@ -154,15 +154,16 @@ int cs_ducy_run_device(CsDucy *d, const float *d_amps, long long namps, long lon
                        void *stream);
 void cs_ducy_free(CsDucy *d);
 
-/* ---- prepsubband's time-domain clipping: decisions only ---------------
+/* ---- prepsubband's time-domain clipping -------------------------------
  * How many spectra PRESTO's clip_times (third_party/presto/src/clipping.c)
  * would replace when the reference's front end runs with -clip clip_sigma
  * (its default, 6) on the 8-bit filterbank at d_raw ([nspec][nchan], SIGPROC
  * order): every full block of L spectra, running statistics carried from
  * block to block.  d_flags (device, nspec / L * L bytes, may be NULL) gets 1
- * for each such spectrum.  The device front end runs without clipping; its
- * output equals the clipped run's exactly when *nclipped is 0 (counted over
- * every full block, also ones a run with a shorter numout never reads).
+ * for each such spectrum.  The unclipped dedispersion equals the clipped
+ * run exactly when *nclipped is 0 (counted over every full block, also ones
+ * a run with a shorter numout never reads); otherwise cs_clip_levels gives
+ * what cs_dedisp_run_device_clipped substitutes.
  * d_scratch: device memory of cs_clip_scratch_bytes(nspec, L) bytes, 256-byte
  * aligned, kept by the caller across calls; NULL makes the call allocate and
  * free its own, which synchronises the device and can take far longer than
@@ -171,6 +172,15 @@ size_t cs_clip_scratch_bytes(long long nspec, int L);
 int cs_clip_count(const uint8_t *d_raw, long long nspec, int nchan, int L, float clip_sigma,
                   long long *nclipped, uint8_t *d_flags, void *d_scratch, size_t scratch_bytes,
                   void *stream, int device);
+
+/* cs_clip_count plus the channel levels clip_times leaves after each block
+ * (its good_chan_levels, clipping.c:118-160), which it writes over the
+ * spectra it replaces: d_levels (device, [nspec / L][nchan] floats, SIGPROC
+ * channel order like d_raw).  d_flags and d_levels are required; with
+ * clip_sigma <= 0 nothing is written.  Returns 0 or -1. */
+int cs_clip_levels(const uint8_t *d_raw, long long nspec, int nchan, int L, float clip_sigma,
+                   long long *nclipped, uint8_t *d_flags, float *d_levels, void *d_scratch,
+                   size_t scratch_bytes, void *stream, int device);
 
 /* ---- SIGPROC filterbank header (in libcoherent_search.so) --------------
  * The header read_filterbank_header parses (third_party/presto/
@@ -228,6 +238,18 @@ long long cs_dedisp_output_length(const CsDedisp *d, long long nspec, long long 
 int cs_dedisp_run_device(CsDedisp *d, const uint8_t *d_raw, long long nspec, long long numout,
                          float *d_out, long long out_stride, void *stream,
                          long long *nout_written);
+
+/* The run prepsubband makes with -clip (its default): the spectra d_flags
+ * marks (cs_clip_levels) take their block's channel levels d_levels, and the
+ * subband and DM sums are evaluated in FP32 in the reference's order
+ * (channels, then subbands, ascending; dispersion.c:245-264, 346-362).  With
+ * no spectrum flagged it equals cs_dedisp_run_device bit for bit.  The first
+ * clipped run allocates the plan's float subbands (nsub x the plan's stride
+ * floats).  Returns 0 or -1. */
+int cs_dedisp_run_device_clipped(CsDedisp *d, const uint8_t *d_raw, long long nspec,
+                                 long long numout, const uint8_t *d_flags, const float *d_levels,
+                                 float *d_out, long long out_stride, void *stream,
+                                 long long *nout_written);
 
 /* Host buffers; copies in and out and waits. */
 int cs_dedisp_run(CsDedisp *d, const uint8_t *h_raw, long long nspec, long long numout,

@@ -123,6 +123,8 @@ typedef struct {
 static float g_clip_sigma;
 static float *g_timemajor, *g_padvals;
 static long long g_nclipped;
+static float *g_levels;             /* optional: clip_times' channel levels per block */
+static long long g_levels_nblocks;
 
 static int read_block(Reader *r, float *chanmajor)
 {
@@ -134,6 +136,8 @@ static int read_block(Reader *r, float *chanmajor)
                 g_timemajor[(long long)t * r->nchan + c] =
                     (float)b[(long long)t * r->nchan + (r->nchan - 1 - c)];
         g_nclipped += clip_times(g_timemajor, r->L, r->nchan, g_clip_sigma, g_padvals, 1);
+        if (g_levels && r->next < g_levels_nblocks)
+            memcpy(g_levels + r->next * r->nchan, g_padvals, sizeof(float) * r->nchan);
         for (int t = 0; t < r->L; t++)
             for (int c = 0; c < r->nchan; c++)
                 chanmajor[(long long)c * r->L + t] = g_timemajor[(long long)t * r->nchan + c];
@@ -213,6 +217,15 @@ int odd_run(const unsigned char *raw, long long nspec, int nchan, int nsub, int 
 }
 
 /* odd_run with prepsubband's -clip clip_sigma; *nclipped = spectra replaced. */
+/* Record, for the next odd_run_clip, the good_chan_levels that clip_times
+ * leaves after each raw block (PRESTO channel order, ascending frequency):
+ * levels[b * nchan + c] for blocks b < nblocks; NULL stops recording. */
+void odd_clip_levels_to(float *levels, long long nblocks)
+{
+    g_levels = levels;
+    g_levels_nblocks = levels ? nblocks : 0;
+}
+
 int odd_run_clip(const unsigned char *raw, long long nspec, int nchan, int nsub, int ndm,
                  int L, int bpr, const int *idispdt, const int *offsets_in, long long numout,
                  float *out, long long out_stride, long long *nout_written, float clip_sigma,

@@ -312,15 +312,18 @@ def _fresh_dedisp_lib() -> C.CDLL:
     lib.odd_run_clip.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_int, C.c_int,
                                  C.c_int, IP, IP, C.c_longlong, C.c_void_p, C.c_longlong,
                                  C.POINTER(C.c_longlong), C.c_float, C.POINTER(C.c_longlong)]
+    lib.odd_clip_levels_to.argtypes = [C.c_void_p, C.c_longlong]
     return lib
 
 
 def ref_dedisp_run(raw, nsub, idisp, offs, L, bpr, numout=-1, clip_sigma=0.0,
-                   return_clipped=False):
+                   return_clipped=False, return_levels=False):
     """The reference's prepsubband output for every DM: [ndm][nout] float32.
     With clip_sigma > 0, PRESTO's clip_times runs on each raw block as
     prepsubband's -clip does; return_clipped adds the number of spectra it
-    replaced."""
+    replaced, return_levels the channel levels it leaves after each block
+    ([nblocks][nchan] float32, ascending frequency; rows of blocks it never
+    read stay NaN)."""
     lib = dedisp_ref_lib() if clip_sigma <= 0 else _fresh_dedisp_lib()
     raw = np.ascontiguousarray(raw, np.uint8)
     nspec, nchan = raw.shape
@@ -332,12 +335,17 @@ def ref_dedisp_run(raw, nsub, idisp, offs, L, bpr, numout=-1, clip_sigma=0.0,
     IP = C.POINTER(C.c_int)
     idisp = np.ascontiguousarray(idisp, np.int32)
     offs = np.ascontiguousarray(offs, np.int32)
+    levels = np.full((max(nspec // L, 1), nchan), np.nan, np.float32)
     if clip_sigma > 0:
+        if return_levels:
+            lib.odd_clip_levels_to(C.c_void_p(levels.ctypes.data), C.c_longlong(nspec // L))
         lib.odd_run_clip(raw.ctypes.data, nspec, nchan, nsub, ndm, L, bpr,
                          idisp.ctypes.data_as(IP), offs.ctypes.data_as(IP), cap, out.ctypes.data,
                          out.shape[1], C.byref(got), float(clip_sigma), C.byref(nclip))
+        lib.odd_clip_levels_to(None, C.c_longlong(0))
     else:
         lib.odd_run(raw.ctypes.data, nspec, nchan, nsub, ndm, L, bpr, idisp.ctypes.data_as(IP),
                     offs.ctypes.data_as(IP), cap, out.ctypes.data, out.shape[1], C.byref(got))
     res = out[:, :got.value]
-    return (res, nclip.value) if return_clipped else res
+    extra = ((nclip.value,) if return_clipped else ()) + ((levels,) if return_levels else ())
+    return (res,) + extra if extra else res

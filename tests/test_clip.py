@@ -73,18 +73,108 @@ def test_clip_count_matches_reference(gpu_ready, geom, nblocks):
         assert dd.clip_count(d.data_ptr(), data.shape[0], 3.0) == want
 
 
+def _device_clipped(dd, t, raw, clip=6.0, numout=-1):
+    """Flags, levels and the clipped dedispersion of raw on the GPU."""
+    import torch
+    L = t.spectra_per_subint
+    nspec = raw.shape[0]
+    nblk = nspec // L
+    d = torch.from_numpy(np.ascontiguousarray(raw)).cuda()
+    flags = torch.full((nblk * L,), 7, dtype=torch.uint8, device="cuda")
+    levels = torch.full((nblk, t.nchan), float("nan"), dtype=torch.float32, device="cuda")
+    n = dd.clip_levels(d.data_ptr(), nspec, flags.data_ptr(), levels.data_ptr(), clip)
+    nout = dd.output_length(nspec, numout)
+    stride = (nout + 3) // 4 * 4
+    out = torch.full((t.ndm, stride), -1.0, dtype=torch.float32, device="cuda")
+    got = dd.run_device_clipped(d.data_ptr(), nspec, flags.data_ptr(), levels.data_ptr(),
+                                out.data_ptr(), stride, numout)
+    torch.cuda.synchronize()
+    assert got == nout
+    return n, flags.cpu().numpy(), levels.cpu().numpy(), out.cpu().numpy()[:, :nout]
+
+
 @pytest.mark.gpu
 @needs_ref
-def test_front_end_refuses_when_clipping_would_act(gpu_ready):
+@pytest.mark.parametrize("geom,nblocks,numout", [("c256_s16_d40", 40, -1),
+                                                 ("c200_s8_d25_cps25", 30, -1),
+                                                 ("c64_s64_d7", 30, -1),
+                                                 ("filterbank_1024x64x500", 8, -1),
+                                                 ("c256_s16_d40", 40, 9000)])
+def test_clipped_dedispersion_matches_reference(gpu_ready, geom, nblocks, numout):
+    """prepsubband -clip on the GPU: the replaced spectra, the channel levels
+    written over them (clip_times' good_chan_levels after every block) and the
+    dedispersed series, all bit for bit against the reference's own run."""
+    g = GEOMS[geom]
+    t = ours_tables(*g)
+    raw = _rfi(fb_for(g, nblocks=nblocks, seed=3), t.spectra_per_subint)
+    want, nref, lev = rb.ref_dedisp_run(raw, t.nsub, t.idispdt, t.offsets, t.spectra_per_subint,
+                                        t.blocks_per_read, numout, clip_sigma=6.0,
+                                        return_clipped=True, return_levels=True)
+    with Dedisperser(t, max_spectra=raw.shape[0]) as dd:
+        n, flags, levels, out = _device_clipped(dd, t, raw, numout=numout)
+    read = ~np.isnan(lev).any(axis=1)                  # blocks the reference read
+    if numout < 0:
+        assert read.all()
+        assert n == nref > 0
+    assert set(np.unique(flags)) <= {0, 1} and int(flags.sum()) == n
+    np.testing.assert_array_equal(levels[:, ::-1][read].view(np.uint32),
+                                  lev[read].view(np.uint32))
+    assert out.shape == want.shape
+    np.testing.assert_array_equal(out.view(np.uint32), want.view(np.uint32))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("geom", sorted(GEOMS))
+def test_clipped_path_without_clips_is_the_integer_path(gpu_ready, geom):
+    """Nothing flagged: the float sums in the reference's order give the
+    integer path's bits (every partial sum is an integer below 2^24)."""
     import torch
-    from coherentsearch_c_b200.prep import PrepSearch
+    g = GEOMS[geom]
+    t = ours_tables(*g)
+    raw = fb_for(g, nblocks=12, seed=5)
+    L = t.spectra_per_subint
+    nspec = raw.shape[0]
+    with Dedisperser(t, max_spectra=nspec) as dd:
+        plain = dd.run(raw)
+        nout = plain.shape[1]
+        stride = (nout + 3) // 4 * 4
+        d = torch.from_numpy(raw).cuda()
+        flags = torch.zeros(nspec // L * L, dtype=torch.uint8, device="cuda")
+        levels = torch.full((nspec // L, t.nchan), 1e30, dtype=torch.float32, device="cuda")
+        out = torch.empty((t.ndm, stride), dtype=torch.float32, device="cuda")
+        assert dd.run_device_clipped(d.data_ptr(), nspec, flags.data_ptr(), levels.data_ptr(),
+                                     out.data_ptr(), stride) == nout
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(out.cpu().numpy()[:, :nout].view(np.uint32),
+                                      plain.view(np.uint32))
+
+
+@pytest.mark.gpu
+@needs_ref
+def test_front_end_clips_like_the_reference(gpu_ready):
+    """PrepSearch with prepsubband's default -clip 6: the padded series of
+    every DM equal the reference's clipped run; with clip_sigma=0 (-noclip)
+    the unclipped one."""
+    import torch
+    from coherentsearch_c_b200.prep import PrepSearch, running_mean
     from coherentsearch_c_b200.search import Options
     g = GEOMS["c256_s16_d40"]
     t = ours_tables(*g)
     raw = _rfi(fb_for(g, nblocks=40, seed=11), t.spectra_per_subint)
-    with PrepSearch(t, raw.shape[0], 24576, g[7], Options(blocksize=4096)) as ps:
-        d = torch.from_numpy(raw).cuda()
-        with pytest.raises(RuntimeError, match="clip"):
+    numout = 24576
+    d = torch.from_numpy(raw).cuda()
+    for clip in (6.0, 0.0):
+        want, nref = rb.ref_dedisp_run(raw, t.nsub, t.idispdt, t.offsets, t.spectra_per_subint,
+                                       t.blocks_per_read, numout, clip_sigma=clip,
+                                       return_clipped=True)
+        with PrepSearch(t, raw.shape[0], numout, g[7], Options(blocksize=4096),
+                        clip_sigma=clip) as ps:
             ps.dedisperse(d.data_ptr(), raw.shape[0])
-    with PrepSearch(t, raw.shape[0], 24576, g[7], Options(blocksize=4096), clip_sigma=0) as ps:
-        ps.dedisperse(d.data_ptr(), raw.shape[0])      # -noclip: runs
+            torch.cuda.synchronize()
+            assert ps.nclipped == nref and (nref > 0) == (clip > 0)
+            got = ps.out.cpu().numpy()
+            nout = want.shape[1]
+            assert ps.nout == nout
+            np.testing.assert_array_equal(got[:, :nout].view(np.uint32), want.view(np.uint32))
+            pad = np.float32(running_mean(want[0]))
+            assert (got[:, nout:ps.N] == pad).all()

@@ -87,19 +87,18 @@ def test_front_end_from_file(gpu_ready, tmp_path):
                             t.spectra_per_subint, t.blocks_per_read, numout)
     d = torch.from_numpy(np.array(data)).cuda()
     # this pulsar is nearly undispersed over 64 MHz, so prepsubband's default
-    # 6-sigma clip would cut it: the front end says so, with the reference's count
-    _, nclip = rb.ref_dedisp_run(np.asarray(data), t.nsub, t.idispdt, t.offsets,
-                                 t.spectra_per_subint, t.blocks_per_read, numout,
-                                 clip_sigma=6.0, return_clipped=True)
+    # 6-sigma clip cuts its pulses: the front end clips them as the reference does
+    refc, nclip = rb.ref_dedisp_run(np.asarray(data), t.nsub, t.idispdt, t.offsets,
+                                    t.spectra_per_subint, t.blocks_per_read, numout,
+                                    clip_sigma=6.0, return_clipped=True)
     assert nclip > 0
-    with PrepSearch(t, h["nspectra"], numout, h["tsamp"], Options(blocksize=4096)) as ps:
-        assert ps.dd.clip_count(d.data_ptr(), h["nspectra"], 6.0) == nclip
-        with pytest.raises(RuntimeError, match="clip"):
+    for clip, want_all in ((6.0, refc), (0.0, ref)):            # -clip 6, -noclip
+        with PrepSearch(t, h["nspectra"], numout, h["tsamp"], Options(blocksize=4096),
+                        clip_sigma=clip) as ps:
             ps.dedisperse(d.data_ptr(), h["nspectra"])
-    with PrepSearch(t, h["nspectra"], numout, h["tsamp"], Options(blocksize=4096),
-                    clip_sigma=0) as ps:                       # -noclip
-        ps.dedisperse(d.data_ptr(), h["nspectra"])
-        pad = np.float32(running_mean(ref[0]))
-        for dm in (0, 5, 11):
-            want = np.concatenate([ref[dm], np.full(numout - ref.shape[1], pad, np.float32)])
-            np.testing.assert_array_equal(ps.series(dm), want)
+            assert ps.nclipped == (nclip if clip else 0)
+            pad = np.float32(running_mean(want_all[0]))
+            for dm in (0, 5, 11):
+                want = np.concatenate([want_all[dm],
+                                       np.full(numout - want_all.shape[1], pad, np.float32)])
+                np.testing.assert_array_equal(ps.series(dm), want)
