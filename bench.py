@@ -439,10 +439,11 @@ def make_filterbank_device(spec, device):
     return raw
 
 
-def dedisp_cpu_rate(raw_host, t, seconds=10.0):
+def dedisp_cpu_rate(raw_host, t, seconds=10.0, clip_sigma=0.0):
     """The reference's dispersion.c kernels under the prepsubband block driver
     (oracle/_ref/libdedisp_ref.so, one thread, as prepsubband runs them) on a
-    bounded stretch of the workload: all DMs over the first blocks."""
+    bounded stretch of the workload: all DMs over the first blocks; with
+    clip_sigma > 0 its clip_times runs on every block first."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import refbind as rb
     nblk = 4 * t.blocks_per_read + 2
@@ -450,7 +451,7 @@ def dedisp_cpu_rate(raw_host, t, seconds=10.0):
     reps, n_out, t0 = 0, 0, time.perf_counter()
     while True:
         out = rb.ref_dedisp_run(sample, t.nsub, t.idispdt, t.offsets, t.spectra_per_subint,
-                                t.blocks_per_read)
+                                t.blocks_per_read, clip_sigma=clip_sigma)
         reps += 1
         n_out += out.shape[0] * out.shape[1]
         if time.perf_counter() - t0 >= seconds:
@@ -484,10 +485,32 @@ def run_dedisp(args):
     # C ABI reads as "the plan's stream"
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
+    L = t.spectra_per_subint
+    nclipped = 0
+    if args.clipped:
+        # RFI that the default 6-sigma clip replaces: every 64th block holds a
+        # broadband burst of 4 spectra, every 97th a dropout spectrum
+        nblk = spec.nspec // L
+        for b in range(1, nblk, 64):
+            raw[b * L + 100: b * L + 104] = 255
+        for b in range(5, nblk, 97):
+            raw[b * L + 7] = 0
+        flags = torch.empty(nblk * L, dtype=torch.uint8, device=dev)
+        levels = torch.empty(nblk * t.nchan, dtype=torch.float32, device=dev)
+        scratch = torch.empty(dd.clip_scratch_bytes(spec.nspec), dtype=torch.uint8, device=dev)
+        torch.cuda.synchronize()
 
     def step():
-        return dd.run_device(raw.data_ptr(), spec.nspec, out.data_ptr(), stride, W["numout"],
-                             stream.cuda_stream)
+        nonlocal nclipped
+        if not args.clipped:
+            return dd.run_device(raw.data_ptr(), spec.nspec, out.data_ptr(), stride,
+                                 W["numout"], stream.cuda_stream)
+        nclipped = dd.clip_levels(raw.data_ptr(), spec.nspec, flags.data_ptr(),
+                                  levels.data_ptr(), 6.0, stream.cuda_stream,
+                                  scratch.data_ptr(), scratch.numel())
+        return dd.run_device_clipped(raw.data_ptr(), spec.nspec, flags.data_ptr(),
+                                     levels.data_ptr(), out.data_ptr(), stride, W["numout"],
+                                     stream.cuda_stream)
 
     for _ in range(args.warmup):
         step()
@@ -525,22 +548,29 @@ def run_dedisp(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8->f32",
         "data": "synthetic",
-        "config": dict(workload=W["workload"], output_per_dm=nout,
-                       blocks_per_read=t.blocks_per_read,
+        "config": dict(workload=W["workload"] + (
+                           "; prepsubband -clip 6 on RFI bursts (4 saturated spectra every 64 "
+                           "blocks, a dropout every 97): clip decisions and levels, then the "
+                           "clipped FP32 dedispersion" if args.clipped else ""),
+                       output_per_dm=nout, blocks_per_read=t.blocks_per_read,
                        l2="inputs larger than L2 (raw input and output both > 126 MB)",
                        parallelism=f"replicas{world}"),
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": (8 if args.clipped else 2) * args.steps,
         "roofline": {"bound": "hbm", "achieved": alg_bytes / (kern_ms * 1e-3) / 1e9,
                      "peak": hbm_peak, "unit": "GB/s",
                      "frac": alg_bytes / (kern_ms * 1e-3) / 1e9 / hbm_peak, "traffic": None,
-                     "kernel": "dd_subband_u8 + dd_dms_u16",
+                     "kernel": ("dd_subband_clip + dd_dms_f32" if args.clipped
+                                else "dd_subband_u8 + dd_dms_u16"),
                      "subband_ms": statistics.mean(sb_ms), "dm_ms": statistics.mean(dm_ms),
                      "peak_kind": f"HBM copy, {peak_kind}",
                      "algorithmic": f"{spec.nspec} x {t.nchan} B raw + {samples} x 4 B output"},
         "clocks": clk.summary(),
     }
+    if args.clipped:
+        line["spectra_clipped"] = nclipped
+        line["clip_levels_ms"] = ms - kern_ms
     # end to end: host (pinned) raw in, host (pinned) output back, through cs_dedisp_run
-    if not args.no_e2e:
+    if not args.no_e2e and not args.clipped:
         h_raw = torch.empty(raw.shape, dtype=torch.uint8, pin_memory=True)
         h_raw.copy_(raw)
         h_out = torch.empty((t.ndm, nout), dtype=torch.float32, pin_memory=True)
@@ -564,7 +594,8 @@ def run_dedisp(args):
         try:
             nblk = 4 * t.blocks_per_read + 2
             host = raw[: nblk * t.spectra_per_subint].cpu().numpy()
-            rate, cores, sample = dedisp_cpu_rate(host, t, seconds=args.cpu_seconds)
+            rate, cores, sample = dedisp_cpu_rate(host, t, seconds=args.cpu_seconds,
+                                                  clip_sigma=6.0 if args.clipped else 0.0)
             line["cpu_baseline"] = {"value": rate, "unit": DEDISP_UNIT, "cores": cores,
                                     "kind": "reference", "sample": sample}
         except Exception as exc:   # noqa: BLE001
@@ -1149,6 +1180,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip the reference's own GPU form (plain single-file baseline)")
+    ap.add_argument("--clipped", action="store_true",
+                    help="dedisp: RFI bursts and prepsubband's -clip 6 path")
     ap.add_argument("--nspec-log2", type=int, default=0,
                     help="dedisp workload length 2^n spectra (default: the 2^22 workload; "
                          "smaller sizes are for profiling captures only)")

@@ -206,6 +206,45 @@ __global__ void chan_sum_kernel(const uint8_t *raw, int L, int nchan, const int 
     sums[b * nchan + c] = (float)s;
 }
 
+/* The same sums with 16-byte loads (nchan a multiple of 16, raw 16-byte
+ * aligned, nchan / 16 <= NT): one CTA per block; thread (row phase p, group g)
+ * adds channels 16g..16g+15 of rows p, p + R, ... and the R row phases are
+ * added in shared memory (integers, so the order does not matter). */
+__global__ void __launch_bounds__(NT) chan_sum16_kernel(const uint8_t *raw, int L, int nchan,
+                                                        const int *zdm, const BlockStats *st,
+                                                        float *sums)
+{
+    extern __shared__ unsigned part[];                /* [R][nchan] */
+    const long long b = blockIdx.x;
+    const int G = nchan >> 4, R = NT / G;
+    const int g = threadIdx.x % G, p = threadIdx.x / G;
+    const float lo = st[b].lo, hi = st[b].hi;
+    unsigned c[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) c[k] = 0;
+    if (p < R) {
+        const uint4 *rows = reinterpret_cast<const uint4 *>(raw + b * L * (long long)nchan) + g;
+        for (int i = p; i < L; i += R) {
+            const float v = (float)zdm[b * L + i];
+            if (!(v > lo && v < hi)) continue;
+            const uint4 w = __ldg(rows + (long long)i * G);
+            const unsigned ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+#pragma unroll
+                for (int k = 0; k < 4; k++) c[4 * q + k] += (ws[q] >> (8 * k)) & 0xffu;
+        }
+#pragma unroll
+        for (int k = 0; k < 16; k++) part[p * nchan + 16 * g + k] = c[k];
+    }
+    __syncthreads();
+    for (int ch = threadIdx.x; ch < nchan; ch += blockDim.x) {
+        unsigned t = 0;
+        for (int q = 0; q < R; q++) t += part[q * nchan + ch];
+        sums[b * nchan + ch] = (float)t;
+    }
+}
+
 /* running channel levels from block to block, in place over the sums (one
  * thread per channel column) */
 __global__ void levels_kernel(const BlockStats *st, long long nblocks, int nchan, float *lv)
@@ -289,7 +328,14 @@ static int clip_run(const uint8_t *d_raw, long long nspec, int nchan, int L, flo
             zdm, n, L, ravg, trig, cnt, d_flags);
         if (d_levels) {
             const dim3 g((unsigned)nblocks, (unsigned)((nchan + ck::NT - 1) / ck::NT));
-            ck::chan_sum_kernel<<<g, ck::NT, 0, st>>>(d_raw, L, nchan, zdm, bs, d_levels);
+            const int G = nchan / 16;
+            if (vec16 && G <= ck::NT) {
+                const size_t psm = (size_t)(ck::NT / G) * nchan * sizeof(unsigned);
+                ck::chan_sum16_kernel<<<(unsigned)nblocks, ck::NT, psm, st>>>(d_raw, L, nchan,
+                                                                            zdm, bs, d_levels);
+            } else {
+                ck::chan_sum_kernel<<<g, ck::NT, 0, st>>>(d_raw, L, nchan, zdm, bs, d_levels);
+            }
             ck::levels_kernel<<<(nchan + ck::NT - 1) / ck::NT, ck::NT, 0, st>>>(bs, nblocks,
                                                                               nchan, d_levels);
         }

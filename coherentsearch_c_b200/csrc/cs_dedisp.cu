@@ -384,21 +384,104 @@ __global__ void __launch_bounds__(256) dd_dms_u16_direct(const DmArgs a)
 
 /* The DM stage of a clipped run: S is float, summed as float_dedisp does
  * (dispersion.c:322-365): from -approx_mean = -0.0f, adding the subbands in
- * ascending order in FP32.  One thread per (DM, sample); the DM index varies
- * fastest over the grid, so CTAs running together read the same stretch of
- * S and share it through L2. */
-__global__ void __launch_bounds__(256) dd_dms_f32(const float *subf, long long sstride, int nsub,
-                                                  int ndm, const int *offs, long long nout,
-                                                  float *out, long long ostride)
+ * ascending order in FP32.  One CTA per (tile of FT samples, group of up to
+ * FG consecutive DMs), the group index fastest over the grid.  The group's
+ * offsets are staged once; then per round of fr subbands the CTA copies, for
+ * each, the union of its DMs' windows (fwin[group][s] = lowest offset, width)
+ * into shared memory with asynchronous copies, one round ahead of the sums
+ * (two buffers).  Each thread adds a subband's term to the FG sums of its FS
+ * samples (t, t + 256, ...), so one broadcast read of a DM's offset serves FS
+ * sums.  S is filled up to sfill samples (every output below nout reads below
+ * it); staged samples from sfill on are zeros and only reach outputs that are
+ * not written. */
+constexpr int FG = 16;          /* DMs per CTA */
+constexpr int FS = 4;           /* samples per thread */
+constexpr int FT = 256 * FS;    /* samples per CTA */
+constexpr int FR = 4;           /* most subbands per round */
+constexpr int FMAXSUB = 256;    /* most subbands (staged offsets) */
+
+static __device__ __forceinline__ void cp_async_commit()
 {
-    const int d = (int)(blockIdx.x % (unsigned)ndm);
-    const long long T = (long long)(blockIdx.x / (unsigned)ndm) * blockDim.x + threadIdx.x;
-    if (T >= nout) return;
-    const int *off = offs + (size_t)d * nsub;
-    float acc = -0.0f;
-    for (int s = 0; s < nsub; s++)
-        acc = __fadd_rn(acc, __ldg(subf + (long long)s * sstride + T + __ldg(off + s)));
-    out[(long long)d * ostride + T] = acc;
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+static __device__ __forceinline__ void cp_async_wait_one()
+{
+    asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(256) dd_dms_f32(const float *subf, long long sstride, int nsub,
+                                                  int ndm, const int *offs, const int2 *fwin,
+                                                  int wmax, int fr, long long sfill,
+                                                  long long nout, float *out, long long ostride)
+{
+    extern __shared__ __align__(16) unsigned char fsm[];
+    int *soff = reinterpret_cast<int *>(fsm);                  /* [nsub][FG], from the window */
+    float *win = reinterpret_cast<float *>(fsm + sizeof(int) * FMAXSUB * FG);  /* [2][fr][wmax] */
+    const unsigned ngrp = (unsigned)((ndm + FG - 1) / FG);
+    const int grp = (int)(blockIdx.x % ngrp);
+    const int d0 = grp * FG;
+    const int nd = min(FG, ndm - d0);
+    const long long T0 = (long long)(blockIdx.x / ngrp) * FT;
+    const int t = threadIdx.x;
+    const int2 *fw = fwin + (size_t)grp * nsub;
+    for (int i = t; i < nsub * FG; i += blockDim.x) {
+        const int sb = i / FG, j = i - sb * FG;
+        soff[i] = j < nd ? offs[(size_t)(d0 + j) * nsub + sb] - fw[sb].x : 0;
+    }
+    /* round r: subbands r*fr .. ; its windows go to buffer r & 1 */
+    auto stage = [&](int r) {
+        float *buf = win + (size_t)(r & 1) * fr * wmax;
+        const int s0 = r * fr, nr = min(fr, nsub - s0);
+        for (int q = 0; q < nr; q++) {
+            const int2 w = fw[s0 + q];
+            const long long first = T0 + w.x;
+            const float *src = subf + (long long)(s0 + q) * sstride + first;
+            for (int i = t; i < w.y; i += blockDim.x) {
+                const bool in = first + i < sfill;
+                cp_async4(buf + q * wmax + i, in ? src + i : subf, in ? 4 : 0);
+            }
+        }
+        cp_async_commit();
+    };
+    float acc[FG][FS];
+#pragma unroll
+    for (int j = 0; j < FG; j++)
+#pragma unroll
+        for (int k = 0; k < FS; k++) acc[j][k] = -0.0f;
+    const int nround = (nsub + fr - 1) / fr;
+    stage(0);
+    for (int r = 0; r < nround; r++) {
+        if (r + 1 < nround) {
+            stage(r + 1);
+            cp_async_wait_one();                      /* round r has landed */
+        } else {
+            cp_async_wait_all();
+        }
+        __syncthreads();
+        const float *buf = win + (size_t)(r & 1) * fr * wmax;
+        const int s0 = r * fr, nr = min(fr, nsub - s0);
+        for (int q = 0; q < nr; q++) {
+            const float *row = buf + q * wmax + t;
+            const int *so = soff + (s0 + q) * FG;
+#pragma unroll
+            for (int j = 0; j < FG; j++) {
+                if (j >= nd) break;
+                const float *rr = row + so[j];
+#pragma unroll
+                for (int k = 0; k < FS; k++) acc[j][k] = __fadd_rn(acc[j][k], rr[256 * k]);
+            }
+        }
+        __syncthreads();                              /* buffer r & 1 is free for round r + 2 */
+    }
+#pragma unroll
+    for (int k = 0; k < FS; k++) {
+        const long long T = T0 + t + 256 * k;
+        if (T >= nout) break;
+#pragma unroll
+        for (int j = 0; j < FG; j++)
+            if (j < nd) out[(long long)(d0 + j) * ostride + T] = acc[j][k];
+    }
 }
 
 }  // namespace dd
@@ -422,6 +505,8 @@ struct CsDedisp {
     long long *d_chunk = nullptr;
     uint16_t *d_sub = nullptr;
     float *d_subf = nullptr;       /* S of clipped runs (allocated by the first one) */
+    int2 *d_fwin = nullptr;        /* clipped DM stage: per (DM group, subband) window */
+    int fwmax = 0;                 /* widest such window (floats) */
     long long sstride = 0;
     uint8_t *d_raw = nullptr;      /* staging for the host-memory entry point */
     float *d_out = nullptr;
@@ -440,6 +525,7 @@ static void dd_release(CsDedisp *D)
     cudaFree(D->d_chunk);
     cudaFree(D->d_sub);
     cudaFree(D->d_subf);
+    cudaFree(D->d_fwin);
     cudaFree(D->d_raw);
     cudaFree(D->d_out);
     if (D->st) cudaStreamDestroy(D->st);
@@ -686,6 +772,27 @@ CS_EXPORT CsDedisp *cs_dedisp_create(int nchan, int nsub, int ndm, const int *id
         DDCK(cudaMemcpy(D->d_nch, nch.data(), sizeof(int) * nch.size(), cudaMemcpyHostToDevice));
     }
     DDCK(cudaMalloc((void **)&D->d_sub, sizeof(uint16_t) * (size_t)nsub * D->sstride));
+    {
+        /* clipped DM stage: the union window of each group of FG DMs per subband */
+        const int ng = (ndm + dd::FG - 1) / dd::FG;
+        std::vector<int2> fw((size_t)ng * nsub);
+        int wmax = 0;
+        for (int g = 0; g < ng; g++)
+            for (int s = 0; s < nsub; s++) {
+                int lo = 1 << 30, hi = 0;
+                for (int d = g * dd::FG; d < std::min(ndm, (g + 1) * dd::FG); d++) {
+                    lo = std::min(lo, offsets[(size_t)d * nsub + s]);
+                    hi = std::max(hi, offsets[(size_t)d * nsub + s]);
+                }
+                fw[(size_t)g * nsub + s] = make_int2(lo, dd::FT + hi - lo);
+                wmax = std::max(wmax, dd::FT + hi - lo);
+            }
+        D->fwmax = wmax;
+        DDCK(cudaMalloc((void **)&D->d_fwin, sizeof(int2) * fw.size()));
+        DDCK(cudaMemcpy(D->d_fwin, fw.data(), sizeof(int2) * fw.size(), cudaMemcpyHostToDevice));
+        DDCK(cudaFuncSetAttribute(dd::dd_dms_f32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  max_optin));
+    }
     DDCK(cudaStreamCreateWithFlags(&D->st, cudaStreamNonBlocking));
     DDCK(cudaEventCreate(&D->ev0));
     DDCK(cudaEventCreate(&D->ev1));
@@ -702,6 +809,26 @@ CS_EXPORT CsDedisp *cs_dedisp_create(int nchan, int nsub, int ndm, const int *id
     DDCK(cudaDeviceSynchronize());
 #undef DDCK
     return D;
+}
+
+/* Dynamic shared memory of the clipped DM stage: the staged offsets and two
+ * rounds of fr windows. */
+static size_t dd_clip_smem(int fr, int fwmax)
+{
+    return sizeof(int) * dd::FMAXSUB * dd::FG + sizeof(float) * 2 * (size_t)fr * fwmax;
+}
+
+/* Subbands the clipped DM stage stages per round (FR, fewer when the
+ * windows are wide); 0 if not even one fits in shared memory, or there are
+ * more subbands than it stages offsets for. */
+static int dd_clip_rounds(const CsDedisp *D)
+{
+    if (D->nsub > dd::FMAXSUB) return 0;
+    int max_optin = 0;
+    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, D->device);
+    for (int fr = dd::FR; fr >= 1; fr--)
+        if (dd_clip_smem(fr, D->fwmax) <= (size_t)max_optin) return fr;
+    return 0;
 }
 
 static cudaError_t dd_enqueue(CsDedisp *D, const uint8_t *d_raw, long long nspec, long long nout,
@@ -747,10 +874,13 @@ static cudaError_t dd_enqueue(CsDedisp *D, const uint8_t *d_raw, long long nspec
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (clip) {
-        const long long ntile = (nout + 255) / 256;
+        const long long ntile = (nout + dd::FT - 1) / dd::FT;
+        const long long ngrp = (D->ndm + dd::FG - 1) / dd::FG;
+        const int fr = dd_clip_rounds(D);
         cudaEventRecord(D->ev1, st);
-        dd::dd_dms_f32<<<(unsigned)(ntile * D->ndm), 256, 0, st>>>(
-            D->d_subf, D->sstride, D->nsub, D->ndm, D->d_offs, nout, d_out, ostride);
+        dd::dd_dms_f32<<<(unsigned)(ntile * ngrp), 256, dd_clip_smem(fr, D->fwmax), st>>>(
+            D->d_subf, D->sstride, D->nsub, D->ndm, D->d_offs, D->d_fwin, D->fwmax, fr, sfill,
+            nout, d_out, ostride);
         cudaEventRecord(D->ev2, st);
         return cudaGetLastError();
     }
@@ -831,9 +961,16 @@ CS_EXPORT int cs_dedisp_run_device_clipped(CsDedisp *D, const uint8_t *d_raw, lo
                         "multiple of 4, the output 16-byte aligned\n", nout);
         return -1;
     }
-    if ((unsigned long long)((nout + 255) / 256) * (unsigned long long)D->ndm >= (1ULL << 31)) {
+    if ((unsigned long long)((nout + dd::FT - 1) / dd::FT) *
+            (unsigned long long)((D->ndm + dd::FG - 1) / dd::FG) >= (1ULL << 31)) {
         fprintf(stderr, "Error: cs_dedisp_run_device_clipped: %lld points x %d DMs is too many "
                         "for one launch\n", nout, D->ndm);
+        return -1;
+    }
+    if (dd_clip_rounds(D) < 1) {
+        fprintf(stderr, "Error: cs_dedisp_run_device_clipped: subband windows of %d samples "
+                        "(%d subbands) need more shared memory than a CTA has\n", D->fwmax,
+                D->nsub);
         return -1;
     }
     if (cudaSetDevice(D->device) != cudaSuccess) return -1;
