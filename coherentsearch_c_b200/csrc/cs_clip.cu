@@ -99,23 +99,18 @@ struct AvgVar {
 
 struct BlockStats {
     int ngood;
+    float med;               /* lower median of the block */
     float lo, hi;            /* good samples lie strictly between */
     double mean, sigma;      /* of the good samples */
 };
 
-/* one CTA per block: lower median by a shared-memory sort, then the two
- * sequential avg_var passes on one thread */
-__global__ void __launch_bounds__(NT) block_kernel(const int *zdm, int L, int P2,
-                                                   BlockStats *out)
+/* one CTA per block: the lower median, by a shared-memory bitonic sort */
+__global__ void __launch_bounds__(NT) median_kernel(const int *zdm, int L, int P2,
+                                                    BlockStats *out)
 {
-    extern __shared__ int sm[];
-    int *x = sm, *srt = sm + L;
+    extern __shared__ int srt[];
     const long long b = blockIdx.x;
-    for (int i = threadIdx.x; i < P2; i += NT) {
-        const int v = i < L ? zdm[b * L + i] : INT_MAX;
-        if (i < L) x[i] = v;
-        srt[i] = v;
-    }
+    for (int i = threadIdx.x; i < P2; i += NT) srt[i] = i < L ? zdm[b * L + i] : INT_MAX;
     __syncthreads();
     for (int k = 2; k <= P2; k <<= 1)
         for (int j = k >> 1; j > 0; j >>= 1) {
@@ -129,50 +124,91 @@ __global__ void __launch_bounds__(NT) block_kernel(const int *zdm, int L, int P2
             }
             __syncthreads();
         }
-    if (threadIdx.x != 0) return;
+    if (threadIdx.x == 0) out[b].med = (float)srt[(L - 1) / 2];
+}
+
+/* one thread per block: the two sequential avg_var passes (all samples, then
+ * the good ones).  Each is a chain of dependent double divisions; running
+ * every block's chain at once keeps the GPU busy where one thread per CTA
+ * would leave the CTA idle.  Samples are read eight at a time, ahead of the
+ * chain. */
+constexpr int ZB = 8;
+__global__ void __launch_bounds__(64) stats_kernel(const int *zdm, int L, long long nblocks,
+                                                   BlockStats *out)
+{
+    const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nblocks) return;
+    const int *x = zdm + b * L;
     AvgVar all;
-    for (int i = 0; i < L; i++) all.push((float)x[i]);
+    for (int i0 = 0; i0 < L; i0 += ZB) {
+        int v[ZB];
+#pragma unroll
+        for (int k = 0; k < ZB; k++) v[k] = i0 + k < L ? __ldg(x + i0 + k) : 0;
+#pragma unroll
+        for (int k = 0; k < ZB; k++)
+            if (i0 + k < L) all.push((float)v[k]);
+    }
     const double sd = sqrt(all.var());
-    const float med = (float)srt[(L - 1) / 2];
+    const float med = out[b].med;
     const float lo = (float)((double)med - 3.0 * sd);
     const float hi = (float)((double)med + 3.0 * sd);
     AvgVar good;
-    for (int i = 0; i < L; i++) {
-        const float v = (float)x[i];
-        if (v > lo && v < hi) good.push(v);
+    for (int i0 = 0; i0 < L; i0 += ZB) {
+        int v[ZB];
+#pragma unroll
+        for (int k = 0; k < ZB; k++) v[k] = i0 + k < L ? __ldg(x + i0 + k) : 0;
+#pragma unroll
+        for (int k = 0; k < ZB; k++) {
+            const float f = (float)v[k];
+            if (i0 + k < L && f > lo && f < hi) good.push(f);
+        }
     }
-    BlockStats s;
+    BlockStats &s = out[b];
     s.lo = lo;
     s.hi = hi;
     s.ngood = (int)good.n;
     s.mean = good.mean;
     s.sigma = good.n ? sqrt(good.var()) : 0.0;
-    out[b] = s;
 }
 
-/* the running mean / sigma from block to block (one thread) */
+/* the running mean / sigma from block to block (one thread; the block
+ * statistics are read eight blocks ahead of the chain) */
 __global__ void running_kernel(const BlockStats *st, long long nblocks, float clip_sigma,
                                float *ravg, float *trig)
 {
     float running_avg = 0.0f, running_std = 0.0f;
-    for (long long b = 0; b < nblocks; b++) {
-        double cur_avg, cur_std;
-        if (st[b].ngood < 1) {
-            cur_avg = (double)running_avg;
-            cur_std = (double)running_std;
-        } else {
-            cur_avg = st[b].mean;
-            cur_std = st[b].sigma;
+    for (long long b0 = 0; b0 < nblocks; b0 += ZB) {
+        int ng[ZB];
+        double mn[ZB], sg[ZB];
+#pragma unroll
+        for (int k = 0; k < ZB; k++)
+            if (b0 + k < nblocks) {
+                ng[k] = st[b0 + k].ngood;
+                mn[k] = st[b0 + k].mean;
+                sg[k] = st[b0 + k].sigma;
+            }
+#pragma unroll
+        for (int k = 0; k < ZB; k++) {
+            const long long b = b0 + k;
+            if (b >= nblocks) break;
+            double cur_avg, cur_std;
+            if (ng[k] < 1) {
+                cur_avg = (double)running_avg;
+                cur_std = (double)running_std;
+            } else {
+                cur_avg = mn[k];
+                cur_std = sg[k];
+            }
+            if (b) {
+                running_avg = (float)(0.9 * (double)running_avg + 0.1 * cur_avg);
+                running_std = (float)(0.9 * (double)running_std + 0.1 * cur_std);
+            } else {
+                running_avg = (float)cur_avg;
+                running_std = (float)cur_std;
+            }
+            ravg[b] = running_avg;
+            trig[b] = clip_sigma * running_std;
         }
-        if (b) {
-            running_avg = (float)(0.9 * (double)running_avg + 0.1 * cur_avg);
-            running_std = (float)(0.9 * (double)running_std + 0.1 * cur_std);
-        } else {
-            running_avg = (float)cur_avg;
-            running_std = (float)cur_std;
-        }
-        ravg[b] = running_avg;
-        trig[b] = clip_sigma * running_std;
     }
 }
 
@@ -252,11 +288,23 @@ __global__ void levels_kernel(const BlockStats *st, long long nblocks, int nchan
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nchan) return;
     float run = 0.0f;
-    for (long long b = 0; b < nblocks; b++) {
-        const int ng = st[b].ngood;
-        const double cur = ng >= 1 ? (double)lv[b * nchan + c] / (double)ng : (double)run;
-        run = b ? (float)(0.9 * (double)run + 0.1 * cur) : (float)cur;
-        lv[b * nchan + c] = run;
+    for (long long b0 = 0; b0 < nblocks; b0 += ZB) {
+        int ng[ZB];
+        float sum[ZB];
+#pragma unroll
+        for (int k = 0; k < ZB; k++)
+            if (b0 + k < nblocks) {
+                ng[k] = st[b0 + k].ngood;
+                sum[k] = lv[(b0 + k) * nchan + c];
+            }
+#pragma unroll
+        for (int k = 0; k < ZB; k++) {
+            const long long b = b0 + k;
+            if (b >= nblocks) break;
+            const double cur = ng[k] >= 1 ? (double)sum[k] / (double)ng[k] : (double)run;
+            run = b ? (float)(0.9 * (double)run + 0.1 * cur) : (float)cur;
+            lv[b * nchan + c] = run;
+        }
     }
 }
 
@@ -297,7 +345,7 @@ static int clip_run(const uint8_t *d_raw, long long nspec, int nchan, int L, flo
     const long long n = nblocks * L;
     int P2 = 1;
     while (P2 < L) P2 <<= 1;
-    const size_t smem = (size_t)(L + P2) * sizeof(int);
+    const size_t smem = (size_t)P2 * sizeof(int);
     size_t off[5];
     const size_t need = clip_layout(nspec, L, off);
     cudaError_t e = cudaSuccess;
@@ -315,14 +363,15 @@ static int clip_run(const uint8_t *d_raw, long long nspec, int nchan, int L, flo
     unsigned long long *cnt = (unsigned long long *)(base + off[4]), hcnt = 0;
     if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st);
     if (e == cudaSuccess && smem > 48 * 1024)
-        e = cudaFuncSetAttribute((const void *)ck::block_kernel,
+        e = cudaFuncSetAttribute((const void *)ck::median_kernel,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) {
         const int vec16 = (nchan % 16 == 0) && (((uintptr_t)d_raw & 15) == 0);
         const long long threads = n * 32;
         ck::zdm_kernel<<<(unsigned)((threads + ck::NT - 1) / ck::NT), ck::NT, 0, st>>>(
             d_raw, n, nchan, vec16, zdm);
-        ck::block_kernel<<<(unsigned)nblocks, ck::NT, smem, st>>>(zdm, L, P2, bs);
+        ck::median_kernel<<<(unsigned)nblocks, ck::NT, smem, st>>>(zdm, L, P2, bs);
+        ck::stats_kernel<<<(unsigned)((nblocks + 63) / 64), 64, 0, st>>>(zdm, L, nblocks, bs);
         ck::running_kernel<<<1, 1, 0, st>>>(bs, nblocks, clip_sigma, ravg, trig);
         ck::decide_kernel<<<(unsigned)((n + ck::NT - 1) / ck::NT), ck::NT, 0, st>>>(
             zdm, n, L, ravg, trig, cnt, d_flags);
