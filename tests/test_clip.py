@@ -17,13 +17,18 @@ def _ref(raw, t, clip):
                              t.blocks_per_read, clip_sigma=clip, return_clipped=True)
 
 
-def _rfi(raw, L):
+def _rfi(raw, L, flat_block=False):
     nb = raw.shape[0] // L
     raw = raw.copy()
     b1, b2, b3 = nb // 6, nb // 2, (5 * nb) // 6
     raw[b1 * L + 100: b1 * L + 104, :] = 255         # a broadband burst of four spectra
     raw[b2 * L + 7, :] = 0                           # a dropout
     raw[b3 * L + 300, ::2] = 255                     # half the band saturated
+    if flat_block:
+        # a whole block of zeros (a receiver dropout): no sample lies strictly
+        # inside median -+ 3 sigma = 0, so the block has no good spectra and
+        # keeps the running statistics and channel levels (clipping.c:139-144)
+        raw[(nb // 3) * L:(nb // 3 + 1) * L, :] = 0
     return raw
 
 
@@ -106,7 +111,8 @@ def test_clipped_dedispersion_matches_reference(gpu_ready, geom, nblocks, numout
     dedispersed series, all bit for bit against the reference's own run."""
     g = GEOMS[geom]
     t = ours_tables(*g)
-    raw = _rfi(fb_for(g, nblocks=nblocks, seed=3), t.spectra_per_subint)
+    raw = _rfi(fb_for(g, nblocks=nblocks, seed=3), t.spectra_per_subint,
+               flat_block=geom != "filterbank_1024x64x500")
     want, nref, lev = rb.ref_dedisp_run(raw, t.nsub, t.idispdt, t.offsets, t.spectra_per_subint,
                                         t.blocks_per_read, numout, clip_sigma=6.0,
                                         return_clipped=True, return_levels=True)
@@ -178,3 +184,34 @@ def test_front_end_clips_like_the_reference(gpu_ready):
             np.testing.assert_array_equal(got[:, :nout].view(np.uint32), want.view(np.uint32))
             pad = np.float32(running_mean(want[0]))
             assert (got[:, nout:ps.N] == pad).all()
+
+
+@pytest.mark.gpu
+def test_clip_levels_edge_cases(gpu_ready):
+    """Less than one block: nothing is decided or written; clip_sigma 0 (-noclip)
+    writes nothing either; a clipped run with no complete output chunk writes no
+    output."""
+    import torch
+    g = GEOMS["c256_s16_d40"]
+    t = ours_tables(*g)
+    L = t.spectra_per_subint
+    raw = fb_for(g, nblocks=3, seed=2)
+    with Dedisperser(t, max_spectra=raw.shape[0]) as dd:
+        d = torch.from_numpy(np.ascontiguousarray(raw)).cuda()
+        flags = torch.full((3 * L,), 7, dtype=torch.uint8, device="cuda")
+        levels = torch.full((3, t.nchan), -1.0, dtype=torch.float32, device="cuda")
+        for nspec, clip in ((L - 1, 6.0), (0, 6.0), (raw.shape[0], 0.0)):
+            assert dd.clip_levels(d.data_ptr(), nspec, flags.data_ptr(), levels.data_ptr(),
+                                  clip) == 0
+        torch.cuda.synchronize()
+        assert (flags.cpu().numpy() == 7).all() and (levels.cpu().numpy() == -1.0).all()
+        # one block: decisions and levels for it, but no output chunk completes
+        assert dd.output_length(L) == 0
+        n = dd.clip_levels(d.data_ptr(), L, flags.data_ptr(), levels.data_ptr(), 6.0)
+        out = torch.full((t.ndm, 4), -1.0, dtype=torch.float32, device="cuda")
+        assert dd.run_device_clipped(d.data_ptr(), L, flags.data_ptr(), levels.data_ptr(),
+                                     out.data_ptr(), 4) == 0
+        torch.cuda.synchronize()
+        assert n == 0 and (out.cpu().numpy() == -1.0).all()
+        assert set(np.unique(flags.cpu().numpy()[:L])) == {0}
+        assert (flags.cpu().numpy()[L:] == 7).all()
