@@ -211,8 +211,8 @@ double cs_prep_pad_value(const float *x, long long n);
  * Input: raw spectra [nspec][nchan] of unsigned 8-bit samples in SIGPROC
  * order (highest frequency first), as the file holds them.  Output: for DM
  * d, out[d * out_stride + t], t < the returned length, bit-identical to the
- * reference's FP32 result for the same delays (no clipping, masking,
- * downsampling or barycentring). */
+ * reference's FP32 result for the same delays (cs_dedisp_run_device_clipped
+ * adds prepsubband's -clip; no masking, downsampling or barycentring). */
 typedef struct CsDedisp CsDedisp;
 
 /* Delay tables as prep_dedisp.c computes them for DMs lodm + i*dmstep:

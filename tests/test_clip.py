@@ -1,6 +1,8 @@
-"""prepsubband's time-domain clipping: the device count of replaced spectra
-(cs_clip_count) against the reference's own clip_times run in the block
-driver, and the front end's refusal when clipping would act."""
+"""prepsubband's time-domain clipping on the device -- the replaced spectra
+(cs_clip_count, cs_clip_levels), the channel levels written over them and the
+clipped dedispersion (cs_dedisp_run_device_clipped) -- against the reference's
+own clip_times run in its block driver, bit for bit, and the front end that
+runs it."""
 import numpy as np
 import pytest
 
