@@ -182,6 +182,10 @@ CS_HIDDEN_API int cs_tables_build(CsTables *t, const FFTFile *ft, const SearchPa
             if (fits) ch->filled |= 1ULL << (h - 1);
         }
         const double rstart = r_lo + (double)ch->i0 * lodr;
+        /* the noise scales depend on the filled set and the slot only, and
+         * consecutive chunks mostly share it (it changes at the harmonic
+         * change points): reuse the previous chunk's, bit for bit */
+        const int same = c > 0 && t->chunks[c - 1].filled == ch->filled;
         for (i = 0; i < t->nslot; i++) {
             const CsSlot *s = &t->slot[i];
             /* src/cuda.cu:1079-1086 / src/search.c:622-629 */
@@ -195,6 +199,10 @@ CS_HIDDEN_API int cs_tables_build(CsTables *t, const FFTFile *ft, const SearchPa
                     else hi = mid;
                 }
                 ch->nvalid[i] = lo;
+            }
+            if (same) {
+                memcpy(ch->invsw[i], t->chunks[c - 1].invsw[i], sizeof(ch->invsw[i]));
+                continue;
             }
             /* src/search.c:851-858, 657-664 */
             const double sig = analytic_sigma(filled, s->k, s->Hk);
