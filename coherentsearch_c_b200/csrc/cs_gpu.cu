@@ -644,6 +644,11 @@ struct GpuSession {
     int *d_tiles;
     uint4 *d_bimg;
     int bbytes;
+    /* what d_bimg holds: the DFT images depend on the harmonic count and the
+     * slot layout only, so a reload with the same layout keeps them */
+    bool img_ok;
+    int img_nh, img_nslot, img_npad, img_kpad;
+    CsSlot img_slot[CS_MAX_SLOT];
     unsigned *d_amax;      /* [2] */
     unsigned *d_count;     /* [1] */
     int *d_err;            /* [1] */
@@ -916,13 +921,24 @@ static int session_load(GpuSession *S, const FFTFile *ft, const SearchParams *p,
     if (t.ntiles > 0)
         CK(cudaMemcpyAsync(S->d_tiles, t.tiles, (size_t)t.ntiles * 3 * sizeof(int), cudaMemcpyHostToDevice, S->st));
     img_halves = (size_t)t.npad * t.kpad;
-    bhi.resize(img_halves);
-    blo.resize(img_halves);
-    cs_tables_dft_images(&S->tab, bhi.data(), blo.data());
-    S->bbytes = (int)(img_halves * 2);
-    CK(dev_reserve((void **)&S->d_bimg, &S->c_bimg, (size_t)2 * S->bbytes));
-    CK(cudaMemcpyAsync(S->d_bimg, bhi.data(), (size_t)S->bbytes, cudaMemcpyHostToDevice, S->st));
-    CK(cudaMemcpyAsync((char *)S->d_bimg + S->bbytes, blo.data(), (size_t)S->bbytes, cudaMemcpyHostToDevice, S->st));
+    if (!(S->img_ok && S->img_nh == t.nh && S->img_nslot == t.nslot && S->img_npad == t.npad &&
+          S->img_kpad == t.kpad &&
+          memcmp(S->img_slot, t.slot, sizeof(CsSlot) * (size_t)t.nslot) == 0)) {
+        S->img_ok = false;
+        bhi.resize(img_halves);
+        blo.resize(img_halves);
+        cs_tables_dft_images(&S->tab, bhi.data(), blo.data());
+        S->bbytes = (int)(img_halves * 2);
+        CK(dev_reserve((void **)&S->d_bimg, &S->c_bimg, (size_t)2 * S->bbytes));
+        CK(cudaMemcpyAsync(S->d_bimg, bhi.data(), (size_t)S->bbytes, cudaMemcpyHostToDevice, S->st));
+        CK(cudaMemcpyAsync((char *)S->d_bimg + S->bbytes, blo.data(), (size_t)S->bbytes, cudaMemcpyHostToDevice, S->st));
+        S->img_ok = true;
+        S->img_nh = t.nh;
+        S->img_nslot = t.nslot;
+        S->img_npad = t.npad;
+        S->img_kpad = t.kpad;
+        memcpy(S->img_slot, t.slot, sizeof(CsSlot) * (size_t)t.nslot);
+    }
     S->use_ws = ws_config(t, total);
     if (S->use_ws && (S->namps >= 2147483000LL || ws_smem(S->use_ws) > S->max_smem))
         S->use_ws = 0;
