@@ -1026,13 +1026,68 @@ fail:
     return NULL;
 }
 
+/* Freed sessions kept for the next create.  The reference's drivers free
+ * their session and build a new one whenever the spectrum length changes
+ * (src/search.c:1388-1406): about twenty device and pinned allocations and
+ * frees per file, each cudaFree waiting for the whole device.  A parked
+ * session keeps its stream, events and grow-only buffers, and the next create
+ * on its device reloads it for the new geometry.  CS_B200_SESSION_PARK sets
+ * how many are kept (default 2; 0 frees at once, as the reference does);
+ * cs_b200_session_park_drain gives their memory back. */
+static std::mutex g_park_mu;
+static std::vector<GpuSession *> g_park;
+
+static size_t park_limit()
+{
+    static const size_t lim = [] {
+        const char *e = getenv("CS_B200_SESSION_PARK");
+        return e ? (size_t)std::max(0, atoi(e)) : (size_t)2;
+    }();
+    return lim;
+}
+
+static GpuSession *park_take(int device)
+{
+    std::lock_guard<std::mutex> g(g_park_mu);
+    for (size_t i = g_park.size(); i-- > 0;) {
+        GpuSession *S = g_park[i];
+        if (S->device == device) {
+            g_park.erase(g_park.begin() + (long)i);
+            return S;
+        }
+    }
+    return nullptr;
+}
+
+CS_EXPORT int cs_b200_session_park_drain(void)
+{
+    std::vector<GpuSession *> all;
+    {
+        std::lock_guard<std::mutex> g(g_park_mu);
+        all.swap(g_park);
+    }
+    for (GpuSession *S : all) {
+        select_device(S->device);
+        session_release(S);
+    }
+    return (int)all.size();
+}
+
 CS_EXPORT GpuSession *cs_gpu_session_create(const FFTFile *ft, const SearchParams *p,
                                             const DirectPlanSet *dplans,
                                             const long long *cstarts, long long total,
                                             int Nprof, long long nchunks, double r_lo,
                                             double lodr, int device)
 {
-    GpuSession *S = session_new(device);
+    GpuSession *S = park_take(device);
+    if (S) {
+        if (select_device(device) != cudaSuccess) {
+            session_release(S);
+            return NULL;
+        }
+    } else {
+        S = session_new(device);
+    }
     if (!S) return NULL;
     if (session_load(S, ft, p, dplans, cstarts, total, Nprof, nchunks, r_lo, lodr) != 0) {
         session_release(S);
@@ -1228,7 +1283,14 @@ CS_EXPORT void cs_gpu_session_free(GpuSession *S)
 {
     if (!S) return;
     select_device(S->device);
-    cudaStreamSynchronize(S->st);
+    if (cudaStreamSynchronize(S->st) == cudaSuccess && park_limit() > 0) {
+        S->p = NULL;                 /* matches nothing until it is reloaded */
+        std::lock_guard<std::mutex> g(g_park_mu);
+        if (g_park.size() < park_limit()) {
+            g_park.push_back(S);
+            return;
+        }
+    }
     session_release(S);
 }
 

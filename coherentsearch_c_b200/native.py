@@ -159,6 +159,8 @@ def declare_gpu_api(lib: C.CDLL) -> C.CDLL:
     lib.cs_b200_session_collapse_wait.restype = C.c_int
     lib.cs_b200_session_sync.argtypes = [C.c_void_p]
     lib.cs_b200_session_sync.restype = C.c_int
+    lib.cs_b200_session_park_drain.argtypes = []
+    lib.cs_b200_session_park_drain.restype = C.c_int
     lib.cs_b200_session_search_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_double,
                                                    C.c_void_p, C.c_longlong,
                                                    P(C.c_longlong), C.c_void_p]

@@ -260,6 +260,17 @@ int cs_dedisp_last_times(CsDedisp *d, float *subband_ms, float *dm_ms);
 
 void cs_dedisp_free(CsDedisp *d);
 
+/* ---- session reuse ---------------------------------------------------
+ * cs_gpu_session_free keeps up to CS_B200_SESSION_PARK freed sessions per
+ * process (default 2; 0 frees at once, as the reference does) and the next
+ * cs_gpu_session_create on the same device reloads one for its geometry,
+ * instead of making and freeing its device and pinned buffers per file (the
+ * reference's drivers free and recreate the session whenever the spectrum
+ * length changes, src/search.c:1388-1406).  Results are the same bits.  A
+ * parked session still holds its device memory; this frees every parked
+ * session and returns how many there were. */
+int cs_b200_session_park_drain(void);
+
 /* ---- search without allocation --------------------------------------
  * No reference counterpart.  cs_gpu_session_run and the enqueue/collect pair
  * may grow the record buffer with cudaMalloc and rerun when more candidates
