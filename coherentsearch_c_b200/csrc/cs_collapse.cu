@@ -37,6 +37,8 @@
  * marked it, as in the host loop.  The FP64 expressions are the host's.
  */
 #include <cuda_runtime.h>
+
+#include <atomic>
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -211,14 +213,38 @@ static __device__ bool related(double r1, double r2, int numharm, double tol)
     return false;
 }
 
-/* remove_harmonics' greedy loop over the metric-ordered list (one CTA) */
+/* remove_harmonics' greedy loop over the metric-ordered list (one CTA).
+ * The walk is serial in the list, so with up to GREEDY_SMEM candidates the
+ * positions' r values and the removal marks are staged in shared memory and
+ * a step costs a shared read, not two dependent global loads; longer lists
+ * walk global memory. */
+constexpr unsigned GREEDY_SMEM = 8192;
 __global__ void __launch_bounds__(1024) greedy_kernel(const unsigned *list, const unsigned *pos,
                                                       const double *r, const unsigned *mp,
                                                       int numharm, double tol,
                                                       unsigned char *removed,
                                                       unsigned char *keep_by_pos)
 {
+    extern __shared__ double gsm[];               /* [GREEDY_SMEM] r, then the marks */
     const unsigned m = *mp;
+    if (m <= GREEDY_SMEM) {
+        double *rs = gsm;
+        unsigned char *rm = reinterpret_cast<unsigned char *>(gsm + GREEDY_SMEM);
+        for (unsigned j = threadIdx.x; j < m; j += blockDim.x) {
+            rs[j] = r[list[pos[j]]];
+            rm[j] = 0;
+        }
+        __syncthreads();
+        for (unsigned i = 0; i < m; i++) {
+            if (rm[i]) continue;                    /* the same value in every thread */
+            const double ri = rs[i];
+            for (unsigned j = i + 1 + threadIdx.x; j < m; j += blockDim.x)
+                if (!rm[j] && related(rs[j], ri, numharm, tol)) rm[j] = 1;
+            __syncthreads();
+        }
+        for (unsigned q = threadIdx.x; q < m; q += blockDim.x) keep_by_pos[pos[q]] = !rm[q];
+        return;
+    }
     for (unsigned j = threadIdx.x; j < m; j += blockDim.x) removed[j] = 0;
     __syncthreads();
     for (unsigned i = 0; i < m; i++) {
@@ -272,6 +298,22 @@ __global__ void emit_kernel(const unsigned *list, const unsigned char *keep, con
 }
 
 }  // namespace cl
+
+/* The greedy kernel's shared-memory limit, raised once per device (the
+ * attribute belongs to the device that is current when it is set). */
+static cudaError_t greedy_prepare(size_t gsmem)
+{
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 64) return e;
+    const unsigned long long bit = 1ULL << dev;
+    if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+    e = cudaFuncSetAttribute((const void *)cl::greedy_kernel,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsmem);
+    if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+}
 
 struct CsCollapse {
     size_t cap;                     /* records */
@@ -479,9 +521,13 @@ int cs_collapse_enqueue(CsCollapse *w, const CsRec *recs, unsigned n, const CsCh
             e = cub::DeviceRadixSort::SortPairsDescending(w->temp, tb, mb, pb, (int)n, 0, 32, st);
         }
         if (e == cudaSuccess) {
-            cl::greedy_kernel<<<1, 1024, 0, st>>>(listp, pb.Current(), w->r, m, numharm,
-                                                  harm_tol, w->removed, w->keep);
-            e = cudaGetLastError();
+            const size_t gsmem = cl::GREEDY_SMEM * (sizeof(double) + 1);
+            e = greedy_prepare(gsmem);
+            if (e == cudaSuccess) {
+                cl::greedy_kernel<<<1, 1024, gsmem, st>>>(listp, pb.Current(), w->r, m, numharm,
+                                                          harm_tol, w->removed, w->keep);
+                e = cudaGetLastError();
+            }
         }
         keep = w->keep;
     }

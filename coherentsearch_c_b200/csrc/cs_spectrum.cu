@@ -67,18 +67,23 @@ __global__ void pack_kernel(const float2 *X, float2 *out, long long n2)
     out[k] = k == 0 ? make_float2(X[0].x, X[n2].x) : X[k];
 }
 
-/* One warp per block: level = (float)(lower median power / ln 2). */
+/* One warp per block: level = (float)(lower median power / ln 2).  The
+ * block's powers (at most MAX_BLOCK, +inf past its end) are sorted by a
+ * bitonic network over the warp -- element 32u + lane in register u of lane
+ * `lane` -- and the (n-1)/2-th is read out: the reference's quickselect
+ * returns the same value. */
 __global__ void block_level_kernel(const float2 *amps, const long long *bstart, const int *blen,
                                    int nblk, double ln2, float *level)
 {
+    constexpr int R = MAX_BLOCK / 32;
     const int b = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (b >= nblk) return;
     const int n = blen[b];
     const float2 *a = amps + bstart[b];
-    float p[MAX_BLOCK / 32];
+    float p[R];
 #pragma unroll
-    for (int u = 0; u < MAX_BLOCK / 32; u++) {
+    for (int u = 0; u < R; u++) {
         const int i = lane + 32 * u;
         p[u] = INFINITY;
         if (i < n) {
@@ -86,28 +91,38 @@ __global__ void block_level_kernel(const float2 *amps, const long long *bstart, 
             p[u] = __fmaf_rn(v.x, v.x, __fmul_rn(v.y, v.y));
         }
     }
-    const int k = (n - 1) / 2;
-    float med = 0.0f;
-    /* element x is the k-th smallest iff #(< x) <= k < #(<= x) */
-    for (int u = 0; u < MAX_BLOCK / 32; u++) {
-        if (32 * u >= n) break;
-        for (int src = 0; src < 32; src++) {
-            if (src + 32 * u >= n) break;
-            const float x = __shfl_sync(0xffffffffu, p[u], src);
-            int lt = 0, le = 0;
 #pragma unroll
-            for (int w = 0; w < MAX_BLOCK / 32; w++) {
-                lt += p[w] < x;
-                le += p[w] <= x;
-            }
+    for (int k = 2; k <= MAX_BLOCK; k <<= 1) {
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                lt += __shfl_xor_sync(0xffffffffu, lt, off);
-                le += __shfl_xor_sync(0xffffffffu, le, off);
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j >= 32) {
+                const int ju = j >> 5;            /* partner register */
+#pragma unroll
+                for (int u = 0; u < R; u++) {
+                    if (u & ju) continue;
+                    const bool asc = ((32 * u + lane) & k) == 0;
+                    const float x = p[u], y = p[u | ju];
+                    p[u] = asc ? fminf(x, y) : fmaxf(x, y);
+                    p[u | ju] = asc ? fmaxf(x, y) : fminf(x, y);
+                }
+            } else {
+                const bool lower = (lane & j) == 0;
+#pragma unroll
+                for (int u = 0; u < R; u++) {
+                    const bool asc = ((32 * u + lane) & k) == 0;
+                    const float x = p[u];
+                    const float y = __shfl_xor_sync(0xffffffffu, x, j);
+                    p[u] = (lower == asc) ? fminf(x, y) : fmaxf(x, y);
+                }
             }
-            if (lt <= k && k < le) med = x;
         }
     }
+    const int k = (n - 1) / 2;
+    float med = p[0];
+#pragma unroll
+    for (int u = 1; u < R; u++)
+        if ((k >> 5) == u) med = p[u];
+    med = __shfl_sync(0xffffffffu, med, k & 31);
     if (lane == 0) level[b] = (float)((double)med / ln2);
 }
 
