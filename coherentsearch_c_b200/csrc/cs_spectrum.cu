@@ -144,18 +144,28 @@ __global__ void normalise_kernel(const float2 *amps, float2 *out, long long n2,
                                  const long long *sstart, const int *slvl, const int *sslope,
                                  int nseg, const float *level, const float *slope)
 {
-    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    /* the segment of the CTA's first bin, found once; a CTA's bins span a
+     * few segments, so each thread walks on from there */
+    __shared__ int seg0;
+    const long long k0 = (long long)blockIdx.x * blockDim.x;
+    if (threadIdx.x == 0) {
+        int lo = 0, hi = nseg - 1;
+        while (lo < hi) {             /* last segment starting at or before k0 */
+            const int mid = (lo + hi + 1) >> 1;
+            if (sstart[mid] <= k0) lo = mid;
+            else hi = mid - 1;
+        }
+        seg0 = lo;
+    }
+    __syncthreads();
+    const long long k = k0 + threadIdx.x;
     if (k >= n2) return;
     if (k == 0) {
         out[0] = make_float2(1.0f, 0.0f);
         return;
     }
-    int lo = 0, hi = nseg - 1;
-    while (lo < hi) {                 /* last segment starting at or before k */
-        const int mid = (lo + hi + 1) >> 1;
-        if (sstart[mid] <= k) lo = mid;
-        else hi = mid - 1;
-    }
+    int lo = seg0;
+    while (lo + 1 < nseg && sstart[lo + 1] <= k) lo++;
     const float lv = level[slvl[lo]];
     float norm;
     if (sslope[lo] < 0) {
