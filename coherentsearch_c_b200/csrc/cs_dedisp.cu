@@ -44,6 +44,17 @@
  *                  reads per subband term.
  *   dd_dms_u16_direct  the same sums straight from L1/L2, for geometries
  *                  whose windows do not fit in shared memory.
+ *
+ * A run with prepsubband's -clip that replaces spectra (cs_clip_levels) has
+ * non-integer channel levels in it, so its sums need FP32 in the reference's
+ * order; S is float there:
+ *   dd_subband_clip  dd_subband_u8's staging plus one clip flag per row;
+ *                  channels added in ascending frequency from 0.0f, a
+ *                  flagged spectrum contributing its block's level.
+ *   dd_dms_f32     one CTA per (1024 samples, 16 DMs); per round of four
+ *                  subbands the union windows are copied into shared memory
+ *                  with cp.async a round ahead of the sums; subbands added in
+ *                  ascending order from -0.0f.
  */
 #include <cuda_runtime.h>
 
