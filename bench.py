@@ -65,7 +65,11 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        # the samples are summarised into the JSON line; the raw file goes to
+        # CS_B200_CLOCKS_DIR when set (to keep it), else the temp directory
+        import tempfile
+        self.path = os.path.join(os.environ.get("CS_B200_CLOCKS_DIR") or tempfile.gettempdir(),
+                                 f"cs_b200_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
