@@ -46,3 +46,29 @@ def test_reloaded_sessions_match_fresh_ones(gpu_ready):
                 np.testing.assert_array_equal(got[f], want[f], err_msg=f)
     assert 1 <= gpu.cs_b200_session_park_drain() <= 2
     assert gpu.cs_b200_session_park_drain() == 0
+
+
+def test_park_off_frees_at_once(gpu_ready):
+    """CS_B200_SESSION_PARK=0: cs_gpu_session_free releases the session, as
+    the reference's does (the limit is read once per process, so a child
+    process runs it)."""
+    import os
+    import subprocess
+    import sys
+    code = (
+        "import numpy as np\n"
+        "from coherentsearch_c_b200 import native as nt\n"
+        "from coherentsearch_c_b200.search import Options, Session\n"
+        "amps = np.ones(1 << 15, np.float32)\n"
+        "for _ in range(3):\n"
+        "    s = Session(1 << 15, 64e-6, Options(nharms=16, blocksize=8192))\n"
+        "    s.run_raw(amps)\n"
+        "    s.close()\n"
+        "print(nt.gpu_lib().cs_b200_session_park_drain())\n")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    for park, want in (("0", "0"), ("1", "1")):
+        env = dict(os.environ, CS_B200_SESSION_PARK=park, PYTHONPATH=root)
+        out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True,
+                             text=True, timeout=300)
+        assert out.returncode == 0, out.stderr
+        assert out.stdout.strip().splitlines()[-1] == want, (park, out.stdout)
