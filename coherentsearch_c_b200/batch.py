@@ -18,6 +18,10 @@ from . import native as nt
 from .search import Options, _as_amps, _file
 
 
+class BatchCancelled(RuntimeError):
+    """The request was cancelled before a slot took it."""
+
+
 class Batch:
     """A pool of search slots on one GPU (cs_gpu_batch_create)."""
 
@@ -53,9 +57,19 @@ class Batch:
         self._keep.pop(rid, None)
         out = nt.candidates_to_numpy(cl)
         self.host.candlist_free(C.byref(cl))
+        if rc == -2:
+            raise BatchCancelled(f"batch request {rid} was cancelled")
         if rc != 0:
             raise RuntimeError(f"batch request {rid} failed (see stderr)")
         return out, q.value, r.value
+
+    def cancel(self, rid: int) -> bool:
+        """Drop a request no slot has taken yet (its wait then raises
+        BatchCancelled); False if it is already running or finished."""
+        rc = self.gpu.cs_gpu_batch_cancel(self.h, rid)
+        if rc < 0:
+            raise KeyError(rid)
+        return rc == 0
 
     def warm(self, N: int, dt: float, opts: Options | None = None) -> None:
         """Load every slot for a length-N search with `opts` (no spectrum is

@@ -1936,6 +1936,25 @@ CS_EXPORT int cs_gpu_batch_wait(CsBatch *B, long long id, CandidateList *out, do
     return status;
 }
 
+CS_EXPORT int cs_gpu_batch_cancel(CsBatch *B, long long id)
+{
+    if (!B) return -1;
+    std::lock_guard<std::mutex> g(B->mu);
+    auto it = B->reqs.find(id);
+    if (it == B->reqs.end()) return -1;          /* unknown, or already waited for */
+    BatchReq *r = it->second;
+    for (auto q = B->queue.begin(); q != B->queue.end(); ++q) {
+        if (*q != r) continue;
+        B->queue.erase(q);
+        r->status = -2;
+        r->t_start = r->t_end = std::chrono::steady_clock::now();
+        r->done = true;
+        B->cv_done.notify_all();
+        return 0;
+    }
+    return 1;                                    /* on a slot or finished */
+}
+
 CS_EXPORT int cs_gpu_batch_warm(CsBatch *B, const FFTFile *ft, const SearchParams *p,
                                 double lofreq, double hifreq, int lobin, int blocksize)
 {

@@ -99,7 +99,7 @@ long long cs_gpu_batch_submit(CsBatch *b, const FFTFile *ft, const SearchParams 
 /* Wait for one request.  *out receives its raw candidates exactly as
  * cs_gpu_session_run returns them (owned by the caller); queued_ms and run_ms
  * (optional) the time it waited for a slot and the time the slot spent on
- * it.  Returns 0, or -1 (unknown id, or the search failed). */
+ * it.  Returns 0, -1 (unknown id, or the search failed) or -2 (cancelled). */
 int cs_gpu_batch_wait(CsBatch *b, long long id, CandidateList *out, double *queued_ms,
                       double *run_ms);
 
@@ -111,6 +111,12 @@ int cs_gpu_batch_wait(CsBatch *b, long long id, CandidateList *out, double *queu
  * searches included.  Returns 0, or -1 if a slot failed. */
 int cs_gpu_batch_warm(CsBatch *b, const FFTFile *ft, const SearchParams *p, double lofreq,
                       double hifreq, int lobin, int blocksize);
+
+/* Cancel a request that no slot has taken yet: it is dropped from the
+ * queue and its wait returns -2 with an empty list.  Returns 0 when
+ * cancelled, 1 when it is already on a slot or finished (it completes as
+ * usual), -1 for an unknown id.  The request still has to be waited for. */
+int cs_gpu_batch_cancel(CsBatch *b, long long id);
 
 /* Requests submitted and not yet waited for. */
 int cs_gpu_batch_pending(CsBatch *b);

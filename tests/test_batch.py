@@ -95,3 +95,25 @@ def test_batch_warm_then_serve(gpu_ready, cases):
         b.warm(1 << 15, DT, opts_for(16))           # smaller: reuses the buffers
         rid = b.submit(cases[0][2], 1 << cases[0][0], DT, opts_for(cases[0][1]))
         same(b.wait(rid)[0], cases[0][3])
+
+
+def test_batch_cancel(gpu_ready, cases):
+    """One slot, many requests: the queued ones can be cancelled (their wait
+    raises BatchCancelled), a finished one cannot, and the others' results do
+    not change."""
+    from coherentsearch_c_b200.batch import BatchCancelled
+    with Batch(nslots=1) as b:
+        ids = [b.submit(amps, 1 << nlog, DT, opts_for(nh)) for nlog, nh, amps, _ in cases]
+        cancelled = [b.cancel(rid) for rid in ids[3:]]
+        assert any(cancelled)                   # the last ones were still queued
+        for rid, (_, _, _, ref), c in zip(ids, cases, [False] * 3 + cancelled):
+            if c:
+                with pytest.raises(BatchCancelled):
+                    b.wait(rid)
+            else:
+                same(b.wait(rid)[0], ref)
+        assert b.pending() == 0
+        rid = b.submit(cases[0][2], 1 << cases[0][0], DT, opts_for(cases[0][1]))
+        same(b.wait(rid)[0], cases[0][3])
+        with pytest.raises(KeyError):
+            b.cancel(rid)                        # already waited for
