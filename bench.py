@@ -962,6 +962,7 @@ def run_serve(args):
             srv.warm(max(lengths), dt, Options(nharms=60, blocksize=65536, threshold=8.0))
             served = run_stream(srv, reqs, arrivals)
             qr = np.array(srv.stats) if srv.stats else np.zeros((1, 2))
+            held = srv.batch.device_bytes()
     with PlainServer() as pl:
         plain = run_stream(pl, reqs, arrivals)
     equal = all(_same_cands(x, y) for x, y in zip(served["results"], plain["results"]))
@@ -988,6 +989,7 @@ def run_serve(args):
                   "p99_ms": plain["p99_ms"], "mean_ms": plain["mean_ms"],
                   "wall_s": plain["wall_s"]},
         "served_vs_plain": served["trials_per_s"] / plain["trials_per_s"],
+        "device_bytes_held": held,
         "equal_candidates": bool(equal), "trials": trials,
         "e2e": {"value": served["trials_per_s"], "unit": UNIT,
                 "h2d_bytes_per_step": int(sum(r.amps.nbytes for r in reqs)),

@@ -86,6 +86,11 @@ class Batch:
                                       opts.lobin, opts.blocksize) != 0:
             raise RuntimeError("cs_gpu_batch_warm failed (see stderr)")
 
+    def device_bytes(self) -> int:
+        """Device memory the slots hold now (what admission keeps within
+        the budget)."""
+        return int(self.gpu.cs_gpu_batch_device_bytes(self.h))
+
     def pending(self) -> int:
         return int(self.gpu.cs_gpu_batch_pending(self.h))
 

@@ -1936,6 +1936,15 @@ CS_EXPORT int cs_gpu_batch_wait(CsBatch *B, long long id, CandidateList *out, do
     return status;
 }
 
+CS_EXPORT long long cs_gpu_batch_device_bytes(CsBatch *B)
+{
+    if (!B) return -1;
+    std::lock_guard<std::mutex> g(B->mu);
+    long long total = 0;
+    for (const BatchSlot &sl : B->slots) total += (long long)sl.bytes;
+    return total;
+}
+
 CS_EXPORT int cs_gpu_batch_cancel(CsBatch *B, long long id)
 {
     if (!B) return -1;

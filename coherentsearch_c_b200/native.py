@@ -176,6 +176,8 @@ def declare_gpu_api(lib: C.CDLL) -> C.CDLL:
     lib.cs_gpu_batch_warm.argtypes = [C.c_void_p, P(FFTFile), P(SearchParams), C.c_double,
                                       C.c_double, C.c_int, C.c_int]
     lib.cs_gpu_batch_warm.restype = C.c_int
+    lib.cs_gpu_batch_device_bytes.argtypes = [C.c_void_p]
+    lib.cs_gpu_batch_device_bytes.restype = C.c_longlong
     lib.cs_gpu_batch_cancel.argtypes = [C.c_void_p, C.c_longlong]
     lib.cs_gpu_batch_cancel.restype = C.c_int
     lib.cs_gpu_batch_pending.argtypes = [C.c_void_p]

@@ -118,6 +118,10 @@ int cs_gpu_batch_warm(CsBatch *b, const FFTFile *ft, const SearchParams *p, doub
  * usual), -1 for an unknown id.  The request still has to be waited for. */
 int cs_gpu_batch_cancel(CsBatch *b, long long id);
 
+/* Device bytes the slots hold now (the figure admission holds to the
+ * budget), or -1. */
+long long cs_gpu_batch_device_bytes(CsBatch *b);
+
 /* Requests submitted and not yet waited for. */
 int cs_gpu_batch_pending(CsBatch *b);
 

@@ -68,10 +68,13 @@ def test_batch_under_memory_budget(gpu_ready, cases):
     """A budget that holds about one request at a time: slots give buffers
     back and wait, and the results do not change."""
     big = max(c[2].nbytes for c in cases)
-    with Batch(nslots=3, mem_budget=big * 3 + (24 << 20)) as b:
+    budget = big * 3 + (24 << 20)
+    with Batch(nslots=3, mem_budget=budget) as b:
+        assert b.device_bytes() == 0
         ids = [b.submit(amps, 1 << nlog, DT, opts_for(nh)) for nlog, nh, amps, _ in cases]
         for rid, (_, _, _, ref) in zip(ids, cases):
             same(b.wait(rid)[0], ref)
+            assert b.device_bytes() > 0         # sessions kept for reuse
 
 
 def test_batch_rejects_request_beyond_budget(gpu_ready, cases):
