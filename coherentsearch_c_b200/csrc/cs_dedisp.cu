@@ -421,7 +421,7 @@ static __device__ __forceinline__ void cp_async_wait_one()
     asm volatile("cp.async.wait_group 1;" ::: "memory");
 }
 
-__global__ void __launch_bounds__(256) dd_dms_f32(const float *subf, long long sstride, int nsub,
+__global__ void __launch_bounds__(256, 3) dd_dms_f32(const float *subf, long long sstride, int nsub,
                                                   int ndm, const int *offs, const int2 *fwin,
                                                   int wmax, int fr, long long sfill,
                                                   long long nout, float *out, long long ostride)
