@@ -6,7 +6,9 @@ produces, under coherentsearch_c_b200/lib/:
   libcsgpu.so            CUDA backend: the reference's cs_gpu_* ABI plus
                          cs_b200.h (self-contained; host helpers hidden)
   libcoherent_search.so  host C: planning, search_file, candidates, .cohout
-  coherent_search, coherent_search_list   the command-line drivers
+The command-line drivers are the reference's own (src/CoherentSearch.c,
+src/list_main.c) linked against these libraries; oracle/Makefile's `dropin`
+target builds them that way for the tests.
 Compiled with nvcc -gencode arch=compute_100a,code=sm_100a -lineinfo; host C
 with -ffp-contract=off (the reference's FP contract, src/Makefile:43).
 """
@@ -106,17 +108,6 @@ def build(verbose: bool = False, force: bool = False) -> None:
     if force or _newer(libhost, host_objs + [libgpu]):
         _run(["gcc", "-shared", "-o", libhost] + host_objs +
              [f"-L{LIB}", "-lcsgpu", "-Wl,-rpath,$ORIGIN", "-lm"], verbose)
-
-    # command-line drivers
-    cli = os.path.join(HOST, "cs_cli.c")
-    if os.path.exists(cli):
-        for name, mode in (("coherent_search", "0"), ("coherent_search_list", "1")):
-            exe = os.path.join(LIB, name)
-            if force or _newer(exe, [cli, libhost] + hdrs):
-                _run(["gcc"] + [f for f in CFLAGS if f != "-fPIC"] +
-                     [f"-DCS_LIST_MODE={mode}", cli, "-o", exe, f"-L{LIB}",
-                      "-lcoherent_search", "-lcsgpu", "-Wl,-rpath,$ORIGIN", "-lpthread",
-                      "-lm"], verbose)
 
 
 if __name__ == "__main__":
