@@ -37,10 +37,18 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = {
     "workload": "precision-study single file: N=2^23 f32 series, dt=64us, nharms=60, m=16, "
-                "hidr=0.5, 0.1-125 Hz, maxdecim 6, blocksize 65536, threshold 8",
-    "N": 1 << 23, "dt": 64e-6, "nharms": 60, "m": 16, "blocksize": 65536,
+                "hidr=0.5, 0.1-125 Hz, maxdecim 6, threshold 8",
+    "N": 1 << 23, "dt": 64e-6, "nharms": 60, "m": 16,
     "l2": "flushed (512 MiB write) before each timed step",
 }
+# Trials per chunk (--blocksize) of each arm.  It sets how the trials are
+# batched, not which trials run or what they give: chunks also break at every
+# harmonic change point, so each chunk's harmonic set, noise scale and
+# candidates are the same at any blocksize.  Each arm runs its own best: the
+# GPU 65536 (the reference's GPU default, src/cli.c:920), the CPU 2048 (2.5x
+# faster than 65536 there, its cache-sized batches).
+BLOCKSIZE_GPU = 65536
+BLOCKSIZE_CPU = 2048
 METRIC = "Fourier trials/sec/GPU"
 UNIT = "trials/s"
 DFT_FLOP_PER_TRIAL = 28560.0      # 2*(2nh-1)*2nh at nh=60 (k | nh folds add none)
@@ -141,7 +149,7 @@ def cpu_reference_rate(amps, N, seconds=10.0, max_reps=50):
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import refbind as rb
     from coherentsearch_c_b200.search import Options
-    opts = Options(blocksize=2048, threshold=8.0)
+    opts = Options(blocksize=BLOCKSIZE_CPU, threshold=8.0)
     _, _, total = opts.geometry(N, WORKLOAD["dt"])
     cores = os.cpu_count() or 1
     rb.ref_lib()
@@ -156,8 +164,52 @@ def cpu_reference_rate(amps, N, seconds=10.0, max_reps=50):
             break
     dt = time.perf_counter() - t0
     sample = (f"{reps} full searches of the workload spectrum ({total} trials each) "
-              f"with the reference CPU path (blocksize 2048, its CPU default)")
+              f"with the reference CPU path (blocksize {BLOCKSIZE_CPU}, its CPU default)")
     return total * reps / dt, cores, sample
+
+
+def precision_study(ses, amps, N, dt, opts, device):
+    """The FP32 search (tensor-core fp16-split DFT) against this repository's
+    FP64 search (--precision f64: FP64 DFT, folds and boxcar), the FP64
+    oracle, on the workload spectrum: relative S/N error of every raw
+    candidate both report, the ones only one reports (threshold flips), and
+    the collapsed list side by side."""
+    from dataclasses import replace
+    from coherentsearch_c_b200.search import Session
+    raw32 = ses.run_raw(amps)
+    s64 = Session(N, dt, replace(opts, precision=1), device=device)
+    try:
+        raw64 = s64.run_raw(amps)
+        s64.enqueue(s64.device_amps_ptr())
+        _, f64_ms, _ = s64.collect()
+        col64 = s64.collapse(raw64)
+    finally:
+        s64.close()
+    col32 = ses.collapse(raw32)
+
+    def keyed(c):
+        return {(round(float(r), 9), int(h)): float(m)
+                for r, h, m in zip(c["r"], c["nharm"], c["metric"])}
+    k32, k64 = keyed(raw32), keyed(raw64)
+    common = sorted(set(k32) & set(k64))
+    rel = np.array([abs(k32[k] - k64[k]) / abs(k64[k]) for k in common]) if common else np.zeros(1)
+    flips = [k32.get(k, k64.get(k)) for k in set(k32) ^ set(k64)]
+    thr = opts.threshold
+    c64 = keyed(col64)
+    table = []
+    for c in col32:
+        k = (round(float(c["r"]), 9), int(c["nharm"]))
+        m64 = c64.get(k)
+        table.append({"freq_hz": round(float(c["freq"]), 9), "nharm": int(c["nharm"]),
+                      "snr_f32": round(float(c["metric"]), 6),
+                      "snr_f64": None if m64 is None else round(m64, 6),
+                      "rel_err": None if m64 is None else abs(float(c["metric"]) - m64) / abs(m64)})
+    return {"oracle": "this repository's --precision f64 search on the GPU",
+            "raw_candidates_f32": int(raw32.size), "raw_candidates_f64": int(raw64.size),
+            "max_rel_snr_err": float(rel.max()), "median_rel_snr_err": float(np.median(rel)),
+            "threshold_flips": len(flips),
+            "flips_outside_1e-3_band": sum(1 for m in flips if abs(m - thr) > 1e-3 * thr),
+            "f64_kernel_ms": f64_ms, "collapsed": table}
 
 
 def ducy_timing(ses, cands, amps, N, dt, reps=3):
@@ -251,12 +303,13 @@ def run_reference(args):
         rates.append(r)
     value = statistics.median(rates)
     from coherentsearch_c_b200.search import Options
-    _, _, total = Options(blocksize=2048).geometry(N, WORKLOAD["dt"])
+    _, _, total = Options(blocksize=BLOCKSIZE_CPU).geometry(N, WORKLOAD["dt"])
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total / value, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": WORKLOAD,
+        "blocksize": BLOCKSIZE_CPU,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -277,7 +330,7 @@ def run_b200(args):
     from coherentsearch_c_b200.search import Options, Session
     amps, N = make_spectrum()
     dt = WORKLOAD["dt"]
-    opts = Options(nharms=60, m=16, blocksize=WORKLOAD["blocksize"], threshold=8.0)
+    opts = Options(nharms=60, m=16, blocksize=BLOCKSIZE_GPU, threshold=8.0)
     ses = Session(N, dt, opts, device=local)
     info = ses.info()
     total = ses.total
@@ -358,13 +411,14 @@ def run_b200(args):
     f_sm = (clocks.get("sm_mhz") or 1965.0) * 1e6
     simt_peak = 148 * 128 * f_sm
     simt_ach = total * SIMT_OPS_PER_TRIAL / (kms * 1e-3)
-    kname = "search_ws60" if info.kernel == 1 else "cs_search_kernel"
+    kname = "search_ws_cfg60" if info.kernel == 1 else "cs_search_kernel"
     traffic = profiled_traffic(kname, total)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic", "config": dict(WORKLOAD, parallelism=f"replicas{world}"),
+        "dtype": "f32", "data": "synthetic", "config": WORKLOAD,
+        "blocksize": BLOCKSIZE_GPU, "replicas": world,
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": int(amps.nbytes),
                 "d2h_bytes_per_step": int(nrec * 16 + 8)},
@@ -390,6 +444,11 @@ def run_b200(args):
         except Exception as exc:   # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0,
                                     "kind": "reference", "sample": f"unavailable: {exc}"}
+    if rank == 0 and world == 1:
+        try:
+            line["precision"] = precision_study(ses, amps, N, dt, opts, local)
+        except Exception as exc:   # noqa: BLE001
+            line["precision"] = {"unavailable": str(exc)}
     if rank == 0 and world == 1:
         try:
             line["ducy"] = ducy_timing(ses, out, amps, N, dt)
@@ -729,7 +788,7 @@ def run_prep(args):
         "gpu_launches": (8 + 16 * t.ndm) * args.steps,
         "roofline": {"bound": "tensor", "achieved": dft_tflops, "peak": tc_peak,
                      "unit": "TFLOP/s", "frac": dft_tflops / tc_peak, "traffic": None,
-                     "kernel": "search_ws60", "kernel_ms_per_dm": kms / t.ndm,
+                     "kernel": "search_ws_cfg60", "kernel_ms_per_dm": kms / t.ndm,
                      "peak_kind": f"bf16 dense, {peak_kind}",
                      "algorithmic": f"{DFT_FLOP_PER_TRIAL:.0f} DFT flop/trial x {total} trials "
                                     f"x {t.ndm} DMs"},
@@ -1109,7 +1168,7 @@ def run_series(args):
         "gpu_launches": 16 * args.steps,     # 4 spectrum, 2 search, 10 collapse (cuFFT, CUB not counted)
         "roofline": {"bound": "tensor", "achieved": dft, "peak": tc_peak, "unit": "TFLOP/s",
                      "frac": dft / tc_peak, "traffic": None,
-                     "kernel": "search_ws60" if ses.info().kernel == 1 else "cs_search_kernel",
+                     "kernel": "search_ws_cfg60" if ses.info().kernel == 1 else "cs_search_kernel",
                      "kernel_ms": kms, "peak_kind": f"bf16 dense, {peak_kind}"},
         "candidates": int(out.size),
         "clocks": clk.summary(),

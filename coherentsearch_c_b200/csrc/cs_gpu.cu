@@ -330,6 +330,59 @@ static __device__ __forceinline__ float scan_widths(const float *ps, int row, in
     return best;
 }
 
+/* The m-tap interpolation of harmonic h of the trial with t*pnum = Q*q + R,
+ * rotated by its phase factor (src/cuda.cu:86-140): the reference's FP32 FMA
+ * chain in tap order, then the unfused rotation, so the amplitude is
+ * bit-identical to the reference's.  Taps outside the spectrum read zero. */
+template <int MT>
+static __device__ __forceinline__ float2 interp_amp(const SearchArgs &args, const CsHarm &hm,
+                                                    int h, int m, long long Q, uint32_t R)
+{
+    uint32_t qd, res;
+    divmod_q((uint32_t)h * R, (uint32_t)args.q, args.qmagic, qd, res);
+    const long long qint = (long long)h * Q + qd;
+    const int ph = args.rowtab[(size_t)(h - 1) * args.q + res];
+    const int row = hm.woff + ph;
+    const long long base = hm.rfloor0 + qint + args.carry[row];
+    const long long b0 = base + 1 - m / 2;
+    const float *wr = args.W + (size_t)row * m;
+    float ar = 0.0f, ai = 0.0f;
+    if (b0 >= 0 && b0 + m <= args.namps) {
+        const float2 *ap = args.amps + b0;
+        if (MT) {
+#pragma unroll
+            for (int i = 0; i < (MT ? MT : 1); i += 4) {
+                const float4 w4 = __ldg(reinterpret_cast<const float4 *>(wr + i));
+                const float2 a0 = __ldg(ap + i), a1 = __ldg(ap + i + 1);
+                const float2 a2 = __ldg(ap + i + 2), a3 = __ldg(ap + i + 3);
+                ar = __fmaf_rn(w4.x, a0.x, ar); ai = __fmaf_rn(w4.x, a0.y, ai);
+                ar = __fmaf_rn(w4.y, a1.x, ar); ai = __fmaf_rn(w4.y, a1.y, ai);
+                ar = __fmaf_rn(w4.z, a2.x, ar); ai = __fmaf_rn(w4.z, a2.y, ai);
+                ar = __fmaf_rn(w4.w, a3.x, ar); ai = __fmaf_rn(w4.w, a3.y, ai);
+            }
+        } else {
+            for (int i = 0; i < m; i++) {
+                const float w = __ldg(wr + i);
+                const float2 a = __ldg(ap + i);
+                ar = __fmaf_rn(w, a.x, ar);
+                ai = __fmaf_rn(w, a.y, ai);
+            }
+        }
+    } else {
+        for (int i = 0; i < m; i++) {
+            const long long idx = b0 + i;
+            float2 a = make_float2(0.0f, 0.0f);
+            if (idx >= 0 && idx < args.namps) a = __ldg(args.amps + idx);
+            const float w = __ldg(wr + i);
+            ar = __fmaf_rn(w, a.x, ar);
+            ai = __fmaf_rn(w, a.y, ai);
+        }
+    }
+    const float2 g = __ldg(args.A + row);
+    return make_float2(__fsub_rn(__fmul_rn(g.x, ar), __fmul_rn(g.y, ai)),
+                       __fadd_rn(__fmul_rn(g.x, ai), __fmul_rn(g.y, ar)));
+}
+
 template <int MT>
 __global__ void __launch_bounds__(CS_NTHREADS, 1)
 cs_search_kernel(const SearchArgs args)
@@ -406,50 +459,9 @@ cs_search_kernel(const SearchArgs args)
                     const int h = 4 * hb + u + 1;
                     float xr = 0.0f, xi = 0.0f;
                     if (valid && h <= nh && ((filled >> (h - 1)) & 1ULL)) {
-                        const CsHarm hm = harm_s[h - 1];
-                        uint32_t qd, res;
-                        divmod_q((uint32_t)h * R, (uint32_t)args.q, args.qmagic, qd, res);
-                        const long long qint = (long long)h * Q + qd;
-                        const int ph = args.rowtab[(size_t)(h - 1) * args.q + res];
-                        const int row = hm.woff + ph;
-                        const long long base = hm.rfloor0 + qint + args.carry[row];
-                        const long long b0 = base + 1 - m / 2;
-                        const float *wr = args.W + (size_t)row * m;
-                        float ar = 0.0f, ai = 0.0f;
-                        if (b0 >= 0 && b0 + m <= args.namps) {
-                            const float2 *ap = args.amps + b0;
-                            if (MT) {
-#pragma unroll
-                                for (int i = 0; i < (MT ? MT : 1); i += 4) {
-                                    const float4 w4 = __ldg(reinterpret_cast<const float4 *>(wr + i));
-                                    const float2 a0 = __ldg(ap + i), a1 = __ldg(ap + i + 1);
-                                    const float2 a2 = __ldg(ap + i + 2), a3 = __ldg(ap + i + 3);
-                                    ar = __fmaf_rn(w4.x, a0.x, ar); ai = __fmaf_rn(w4.x, a0.y, ai);
-                                    ar = __fmaf_rn(w4.y, a1.x, ar); ai = __fmaf_rn(w4.y, a1.y, ai);
-                                    ar = __fmaf_rn(w4.z, a2.x, ar); ai = __fmaf_rn(w4.z, a2.y, ai);
-                                    ar = __fmaf_rn(w4.w, a3.x, ar); ai = __fmaf_rn(w4.w, a3.y, ai);
-                                }
-                            } else {
-                                for (int i = 0; i < m; i++) {
-                                    const float w = __ldg(wr + i);
-                                    const float2 a = __ldg(ap + i);
-                                    ar = __fmaf_rn(w, a.x, ar);
-                                    ai = __fmaf_rn(w, a.y, ai);
-                                }
-                            }
-                        } else {
-                            for (int i = 0; i < m; i++) {
-                                const long long idx = b0 + i;
-                                float2 a = make_float2(0.0f, 0.0f);
-                                if (idx >= 0 && idx < args.namps) a = __ldg(args.amps + idx);
-                                const float w = __ldg(wr + i);
-                                ar = __fmaf_rn(w, a.x, ar);
-                                ai = __fmaf_rn(w, a.y, ai);
-                            }
-                        }
-                        const float2 g = __ldg(args.A + row);
-                        xr = __fsub_rn(__fmul_rn(g.x, ar), __fmul_rn(g.y, ai));
-                        xi = __fadd_rn(__fmul_rn(g.x, ai), __fmul_rn(g.y, ar));
+                        const float2 x = interp_amp<MT>(args, harm_s[h - 1], h, m, Q, R);
+                        xr = x.x;
+                        xi = x.y;
                     }
                     /* split the scaled amplitude into fp16 hi + lo */
                     const float sr = xr * scale, si = xi * scale;
@@ -605,6 +617,7 @@ cs_search_kernel(const SearchArgs args)
 }
 
 #include "cs_search_ws.cuh"
+#include "cs_search_f64.cuh"
 #include "cs_collapse.h"
 
 /* ------------------------------------------------------------------ */
@@ -666,8 +679,17 @@ struct GpuSession {
     float4 *d_AC;
     wsk::Harm *d_harm2;
     wsk::Harm hh[wsk::MAX_NH];
+    /* FP64 search (p->precision == CS_PREC_F64) */
+    int prec64;
+    f64k::Extra fx;
+    int f64_smem;
+    double *d_bcs, *d_scales;
+    CsRec64 *d_recs64;
+    unsigned cap64;
+    CsRec64 *h_recs64;     /* pinned record staging */
+    size_t h_recs64_cap;
     /* capacities (bytes) of the buffers session_load may reuse */
-    size_t c_amps, c_rowtab, c_W, c_A, c_carry, c_chunks, c_tiles, c_bimg;
+    size_t c_amps, c_rowtab, c_W, c_A, c_carry, c_chunks, c_tiles, c_bimg, c_bcs, c_scales;
 };
 
 static cudaError_t select_device(int device)
@@ -734,6 +756,10 @@ static void session_release(GpuSession *S)
     cudaFree(S->d_Wt);
     cudaFree(S->d_AC);
     cudaFree(S->d_harm2);
+    cudaFree(S->d_bcs);
+    cudaFree(S->d_scales);
+    cudaFree(S->d_recs64);
+    if (S->h_recs64) cudaFreeHost(S->h_recs64);
     if (S->h_count) cudaFreeHost(S->h_count);
     if (S->h_recs) cudaFreeHost(S->h_recs);
     cs_collapse_free(S->coll);
@@ -769,6 +795,19 @@ static int tmem_columns(const CsTables &t)
     int nc = 32;
     while (nc < need) nc <<= 1;
     return nc;
+}
+
+static int grow_records64(GpuSession *S, unsigned cap)
+{
+    cudaFree(S->d_recs64);
+    S->d_recs64 = NULL;
+    S->cap64 = 0;
+    if (cudaMalloc((void **)&S->d_recs64, (size_t)cap * sizeof(CsRec64)) != cudaSuccess) {
+        fprintf(stderr, "Error: cannot allocate %u FP64 candidate records on the GPU\n", cap);
+        return -1;
+    }
+    S->cap64 = cap;
+    return 0;
 }
 
 static int grow_records(GpuSession *S, unsigned cap)
@@ -939,7 +978,47 @@ static int session_load(GpuSession *S, const FFTFile *ft, const SearchParams *p,
         S->img_kpad = t.kpad;
         memcpy(S->img_slot, t.slot, sizeof(CsSlot) * (size_t)t.nslot);
     }
-    S->use_ws = ws_config(t, total);
+    S->prec64 = t.prec64;
+    if (S->prec64) {
+        /* FP64 profile stage: half-spectrum DFT tables, per-chunk FP64 noise
+         * scales, prefix-sum layout (cs_search_f64.cuh) */
+        f64k::Extra &x = S->fx;
+        memset(&x, 0, sizeof(x));
+        x.nunit = cs_tables_f64_units(&t);
+        x.ucols = (x.nunit + 3) / 4 * 4;
+        std::vector<double> bcs((size_t)2 * t.nh * x.ucols);
+        cs_tables_dft_f64(&t, bcs.data(), bcs.data() + (size_t)t.nh * x.ucols, x.ucols, x.unit0);
+        x.prs = t.ncol | 1;
+        int off = 0;
+        for (int q = 0; q < t.nslot; q++) {
+            x.ps_off[q] = off;
+            off += f64k::TT * (t.slot[q].nk + t.slot[q].wmax + 1);
+        }
+        x.ps_total = off;
+        S->f64_smem = f64k::smem_bytes(t.nh, x.ucols, x.prs, x.ps_total);
+        if (S->f64_smem + (int)sizeof(CsHarm) * CS_MAX_NH > S->max_smem) {
+            fprintf(stderr, "Error: the FP64 search needs %d bytes of shared memory, device "
+                            "%d allows %d\n", S->f64_smem, S->device, S->max_smem);
+            return -1;
+        }
+        CK(dev_reserve((void **)&S->d_bcs, &S->c_bcs, bcs.size() * sizeof(double)));
+        CK(cudaMemcpyAsync(S->d_bcs, bcs.data(), bcs.size() * sizeof(double),
+                           cudaMemcpyHostToDevice, S->st));
+        const size_t nsc = (size_t)(nchunks > 0 ? nchunks : 1) * CS_F64_SCALES;
+        CK(dev_reserve((void **)&S->d_scales, &S->c_scales, nsc * sizeof(double)));
+        CK(cudaMemcpyAsync(S->d_scales, t.invsw64, nsc * sizeof(double), cudaMemcpyHostToDevice,
+                           S->st));
+        x.bcs = S->d_bcs;
+        x.scales = S->d_scales;
+        long long want = (total * t.nslot) / 16 + 4096;
+        if (want > (long long)0x7fffffff) want = 0x7fffffff;
+        if (!S->d_recs64 || S->cap64 < (unsigned)want)
+            if (grow_records64(S, (unsigned)want) != 0) return -1;
+        x.recs = S->d_recs64;
+        CK(set_smem_cap((const void *)f64k::search_f64<16>, S->max_smem));
+        CK(set_smem_cap((const void *)f64k::search_f64<0>, S->max_smem));
+    }
+    S->use_ws = S->prec64 ? 0 : ws_config(t, total);
     if (S->use_ws && (S->namps >= 2147483000LL || ws_smem(S->use_ws) > S->max_smem))
         S->use_ws = 0;
     if (S->use_ws) {
@@ -994,6 +1073,7 @@ static size_t session_bytes(const GpuSession *S)
 {
     return S->c_amps + S->c_rowtab + S->c_W + S->c_A + S->c_carry + S->c_chunks + S->c_tiles +
            S->c_bimg + (size_t)S->cap * sizeof(CsRec) + sizeof(CsHarm) * CS_MAX_NH +
+           S->c_bcs + S->c_scales + (size_t)S->cap64 * sizeof(CsRec64) +
            (S->d_Wt ? (size_t)wsk::MAX_NH * 4 * wsk::WT_STRIDE * sizeof(float4) : 0);
 }
 
@@ -1156,6 +1236,21 @@ static cudaError_t enqueue_search(GpuSession *S, const float2 *d_amps, double th
         cs_amax_kernel<<<g, 256, 0, S->st>>>(d_amps, S->namps, S->d_amax);
     }
     if (S->tab.ntiles <= 0) return cudaGetLastError();
+    if (S->prec64) {
+        SearchArgs a64 = make_args(S, d_amps, threshold);
+        a64.cap = S->cap64;
+        f64k::Extra x = S->fx;
+        x.recs = S->d_recs64;
+        const int nsub = S->tab.ntiles * (CS_TILE_M / f64k::TT);
+        const int grid = std::min(nsub, S->nsm);
+        if (timed) cudaEventRecord(S->ev0, S->st);
+        if (S->tab.m == 16)
+            f64k::search_f64<16><<<grid, f64k::NT, S->f64_smem, S->st>>>(a64, x);
+        else
+            f64k::search_f64<0><<<grid, f64k::NT, S->f64_smem, S->st>>>(a64, x);
+        if (timed) cudaEventRecord(S->ev1, S->st);
+        return cudaGetLastError();
+    }
     if (S->use_ws) {
         wsk::Args w;
         memset(&w, 0, sizeof(w));
@@ -1196,6 +1291,42 @@ static cudaError_t enqueue_search(GpuSession *S, const float2 *d_amps, double th
     return cudaGetLastError();
 }
 
+/* The FP64 search's records: grow and rerun on overflow, else read back,
+ * order and harvest them. */
+static int collect64(GpuSession *S, unsigned n, double threshold, CandidateList *out,
+                     int *need_rerun)
+{
+    cudaError_t e;
+    if (n > S->cap64) {
+        if (grow_records64(S, n + n / 8 + 1024) != 0) return -1;
+        *need_rerun = 1;
+        return 0;
+    }
+    if (n == 0) return 0;
+    if ((size_t)n > S->h_recs64_cap) {
+        const size_t cap = (size_t)n + n / 4 + 1024;
+        if (S->h_recs64) cudaFreeHost(S->h_recs64);
+        S->h_recs64 = NULL;
+        S->h_recs64_cap = 0;
+        if ((e = cudaMallocHost((void **)&S->h_recs64, cap * sizeof(CsRec64))) != cudaSuccess) {
+            S->h_recs64 = NULL;
+            fprintf(stderr, "Error: B200 record staging: %s\n", cudaGetErrorString(e));
+            return -1;
+        }
+        S->h_recs64_cap = cap;
+    }
+    if ((e = cudaMemcpyAsync(S->h_recs64, S->d_recs64, (size_t)n * sizeof(CsRec64),
+                             cudaMemcpyDeviceToHost, S->st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(S->st)) != cudaSuccess) {
+        fprintf(stderr, "Error: B200 search readback failed: %s\n", cudaGetErrorString(e));
+        return -1;
+    }
+    cs_sort_records64(S->h_recs64, (long long)n);
+    cs_harvest64(&S->tab, S->h_recs64, (long long)n, S->r_lo, S->lodr, (double)S->N, S->T,
+                 threshold, out);
+    return 0;
+}
+
 /* Read back the records and build the candidate list. */
 static int collect(GpuSession *S, double threshold, CandidateList *out, int *need_rerun)
 {
@@ -1214,6 +1345,7 @@ static int collect(GpuSession *S, double threshold, CandidateList *out, int *nee
         return -1;
     }
     const unsigned n = S->h_count[0];
+    if (S->prec64) return collect64(S, n, threshold, out, need_rerun);
     if (n > S->cap) {
         if (grow_records(S, n + n / 8 + 1024) != 0) return -1;
         *need_rerun = 1;
@@ -1324,9 +1456,9 @@ CS_EXPORT int cs_b200_session_info(const GpuSession *S, CsB200Info *info)
     info->nslot = S->tab.nslot;
     info->npad = S->tab.npad;
     info->kpad = S->tab.kpad;
-    info->smem_bytes = S->use_ws ? ws_smem(S->use_ws) : smem_bytes(S->tab);
+    info->smem_bytes = S->prec64 ? S->f64_smem : S->use_ws ? ws_smem(S->use_ws) : smem_bytes(S->tab);
     info->grid = std::min(S->tab.ntiles, S->nsm);
-    info->kernel = S->use_ws ? 1 : 0;
+    info->kernel = S->prec64 ? 2 : S->use_ws ? 1 : 0;
     info->total = S->total;
     info->rec_capacity = S->cap;
     return 0;
@@ -1367,6 +1499,11 @@ CS_EXPORT int cs_b200_session_collapse_enqueue(GpuSession *S, double threshold, 
                                                double harm_tol)
 {
     if (!S) return -1;
+    if (S->prec64) {
+        fprintf(stderr, "Error: the device collapse takes FP32 sessions; collect an FP64 "
+                        "search with cs_b200_session_collect\n");
+        return -1;
+    }
     cudaError_t e;
     if ((e = cudaMemcpyAsync(S->h_count, S->d_count, sizeof(unsigned), cudaMemcpyDeviceToHost,
                              S->st)) != cudaSuccess ||
@@ -1527,6 +1664,10 @@ CS_EXPORT int cs_b200_session_search_noalloc(GpuSession *S, const float *d_amps,
 {
     if (nout) *nout = 0;
     if (!S || !out || !nout || cap < 0) return -1;
+    if (S->prec64) {
+        fprintf(stderr, "Error: the allocation-free search takes FP32 sessions\n");
+        return -1;
+    }
     if (select_device(S->device) != cudaSuccess) return -1;
     unsigned char *base = noalloc_scratch(S->device);
     if (!base) return -1;

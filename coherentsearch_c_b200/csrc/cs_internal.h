@@ -54,6 +54,19 @@ typedef struct {
     float metric;
 } CsRec;
 
+/* Candidate record of the FP64 search (--precision f64). */
+typedef struct {
+    int chunk;
+    int slot;
+    int j;
+    int pad;
+    double metric;
+} CsRec64;
+
+/* Per chunk, per slot of the FP64 search: invsigma = 1/sigma in double,
+ * then invsigma * shape[w] for each width (src/search.c:649-656). */
+#define CS_F64_SCALES (CS_MAX_SLOT * (CS_NWMAX + 1))
+
 /* Everything the host builds once per session geometry. */
 typedef struct {
     int nh, m, q, pnum;
@@ -85,6 +98,10 @@ typedef struct {
      * res = (t*h*pnum) mod q the phase offset dr0 + res/q reaches 1 exactly
      * when res >= carry_res[h] (monotone in res; src/interp.c:260-262) */
     int carry_res[CS_MAX_NH];
+    /* FP64 search only (p->precision == CS_PREC_F64): CS_F64_SCALES doubles
+     * per chunk, [slot][0] = invsigma, [slot][1 + w] = invsw of width w */
+    int prec64;
+    double *invsw64;
 } CsTables;
 
 /* Build / free the tables.  Returns 0 or -1 with a message in err. */
@@ -100,6 +117,21 @@ void cs_tables_free(CsTables *t);
  * npad*kpad halves, returned as raw 16-bit patterns. */
 void cs_tables_dft_images(const CsTables *t, uint16_t *bhi, uint16_t *blo);
 
+/* The half-spectrum DFT of the FP64 search.  Each profile-producing slot
+ * (the base and every decimation that does not fold) owns Hk+1 units, one per
+ * output bin n = 0..Hk; for harmonic h (row h-1) and unit u,
+ *   bc[(h-1)*ucols + u] = c2r cosine weight of bin n  (2 cos, or cos(pi n) at
+ *                         the sub-stack's Nyquist harmonic),
+ *   bs[(h-1)*ucols + u] = 2 sin(2 pi j n / 2Hk), zero at n = 0, Hk and for the
+ *                         Nyquist harmonic,
+ * so that with C = sum_h Re X_h bc and S = sum_h Im X_h bs the profile is
+ * x[n] = C - S and x[2Hk - n] = C + S (0 < n < Hk).  unit0[s] is the slot's
+ * first unit, or -1 for a folded slot.  Returns the unit count; bc and bs
+ * hold nh * ucols doubles each (ucols = units rounded up to 4). */
+int  cs_tables_dft_f64(const CsTables *t, double *bc, double *bs, int ucols,
+                       int unit0[CS_MAX_SLOT]);
+int  cs_tables_f64_units(const CsTables *t);
+
 /* Turn sorted records into the reference's Candidate list
  * (src/cuda.cu:837-881 arithmetic). */
 void cs_harvest(const CsTables *t, const CsRec *recs, long long n,
@@ -108,6 +140,12 @@ void cs_harvest(const CsTables *t, const CsRec *recs, long long n,
 
 /* Sort records by (chunk, slot, j). */
 void cs_sort_records(CsRec *recs, long long n);
+
+/* The same for FP64 records. */
+void cs_sort_records64(CsRec64 *recs, long long n);
+void cs_harvest64(const CsTables *t, const CsRec64 *recs, long long n,
+                  double r_lo, double lodr, double N, double T,
+                  double threshold, CandidateList *out);
 
 #ifdef __cplusplus
 }

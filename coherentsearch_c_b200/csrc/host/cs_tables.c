@@ -70,6 +70,7 @@ CS_HIDDEN_API void cs_tables_free(CsTables *t)
     free(t->rowtab);
     free(t->Wt);
     free(t->AC);
+    free(t->invsw64);
     memset(t, 0, sizeof(*t));
 }
 
@@ -162,6 +163,12 @@ CS_HIDDEN_API int cs_tables_build(CsTables *t, const FFTFile *ft, const SearchPa
     t->nchunks = nchunks;
     t->chunks = (CsChunk *)calloc((size_t)(nchunks ? nchunks : 1), sizeof(CsChunk));
     if (!t->chunks) { snprintf(err, errlen, "out of host memory"); return -1; }
+    t->prec64 = p->precision == CS_PREC_F64;
+    if (t->prec64) {
+        t->invsw64 = (double *)calloc((size_t)(nchunks ? nchunks : 1) * CS_F64_SCALES,
+                                      sizeof(double));
+        if (!t->invsw64) { snprintf(err, errlen, "out of host memory"); return -1; }
+    }
     const double nyq = (double)ft->N / 2.0;
     uint8_t filled[CS_MAX_NH];
     long long c;
@@ -202,6 +209,10 @@ CS_HIDDEN_API int cs_tables_build(CsTables *t, const FFTFile *ft, const SearchPa
             }
             if (same) {
                 memcpy(ch->invsw[i], t->chunks[c - 1].invsw[i], sizeof(ch->invsw[i]));
+                if (t->prec64)
+                    memcpy(t->invsw64 + (size_t)c * CS_F64_SCALES + i * (CS_NWMAX + 1),
+                           t->invsw64 + (size_t)(c - 1) * CS_F64_SCALES + i * (CS_NWMAX + 1),
+                           (CS_NWMAX + 1) * sizeof(double));
                 continue;
             }
             /* src/search.c:851-858, 657-664 */
@@ -213,6 +224,13 @@ CS_HIDDEN_API int cs_tables_build(CsTables *t, const FFTFile *ft, const SearchPa
             int w;
             for (w = 0; w < s->nw; w++)
                 ch->invsw[i][w] = (float)((double)invsigma * shape[w]);
+            if (t->prec64) {
+                /* the FP64 path keeps sigma in double (src/search.c:649-651) */
+                double *d = t->invsw64 + (size_t)c * CS_F64_SCALES + i * (CS_NWMAX + 1);
+                const double inv64 = sig > 0.0 ? 1.0 / sig : 0.0;
+                d[0] = inv64;
+                for (w = 0; w < s->nw; w++) d[1 + w] = inv64 * shape[w];
+            }
         }
     }
     t->ntiles = ntiles;
@@ -378,6 +396,43 @@ CS_HIDDEN_API void cs_tables_dft_images(const CsTables *t, uint16_t *bhi, uint16
     }
 }
 
+CS_HIDDEN_API int cs_tables_f64_units(const CsTables *t)
+{
+    int s, u = 0;
+    for (s = 0; s < t->nslot; s++)
+        if (t->slot[s].col0 >= 0) u += t->slot[s].Hk + 1;
+    return u;
+}
+
+CS_HIDDEN_API int cs_tables_dft_f64(const CsTables *t, double *bc, double *bs, int ucols,
+                                    int unit0[CS_MAX_SLOT])
+{
+    const int nh = t->nh;
+    memset(bc, 0, (size_t)nh * ucols * sizeof(double));
+    memset(bs, 0, (size_t)nh * ucols * sizeof(double));
+    int s, n, h, u = 0;
+    for (s = 0; s < CS_MAX_SLOT; s++) unit0[s] = -1;
+    for (s = 0; s < t->nslot; s++) {
+        const CsSlot *sl = &t->slot[s];
+        if (sl->col0 < 0) continue;           /* folded from the base profile */
+        const int k = sl->k, Hk = sl->Hk;
+        unit0[s] = u;
+        for (n = 0; n <= Hk; n++, u++) {
+            for (h = 1; h <= nh; h++) {
+                if (h % k) continue;
+                const int j = h / k;
+                if (j > Hk) continue;
+                double cre, cim;
+                c2r_coeff(j, Hk, n, &cre, &cim);
+                bc[(size_t)(h - 1) * ucols + u] = cre;
+                /* x[n] = C - S: S carries +2 sin, the negation of cim */
+                bs[(size_t)(h - 1) * ucols + u] = (n == 0 || n == Hk || j == Hk) ? 0.0 : -cim;
+            }
+        }
+    }
+    return u;
+}
+
 static int rec_cmp(const void *a, const void *b)
 {
     const CsRec *x = (const CsRec *)a, *y = (const CsRec *)b;
@@ -453,28 +508,63 @@ CS_HIDDEN_API void cs_sort_records(CsRec *recs, long long n)
     free(tmp);
 }
 
+/* One record -> Candidate (src/cuda.cu:837-881 arithmetic); false when it
+ * is not reported (below the threshold, or a decimated trial at or past the
+ * Nyquist frequency). */
+static int harvest_one(const CsTables *t, int chunk, int slot, int j, double metric,
+                       double r_lo, double lodr, double nyq, double T, double threshold,
+                       Candidate *cd)
+{
+    if (!(metric > threshold)) return 0;
+    const CsSlot *s = &t->slot[slot];
+    const double rstart = r_lo + (double)t->chunks[chunk].i0 * lodr;
+    const double rfreq = rstart + (double)j * lodr;
+    const double kmul = (double)s->k;
+    const double rsel = kmul != 1.0 ? kmul * rfreq : rfreq;
+    if (slot != 0 && !(rsel < nyq)) return 0;
+    cd->freq = rsel / T;
+    cd->metric = metric;
+    cd->r = rsel;
+    cd->nharm = s->Hk;
+    cd->ducy = NAN;
+    return 1;
+}
+
 CS_HIDDEN_API void cs_harvest(const CsTables *t, const CsRec *recs, long long n,
                               double r_lo, double lodr, double N, double T,
                               double threshold, CandidateList *out)
 {
-    const double nyq = N / 2.0;
     long long i;
-    for (i = 0; i < n; i++) {
-        const CsRec *r = &recs[i];
-        const double metric = (double)r->metric;
-        if (!(metric > threshold)) continue;
-        const CsSlot *s = &t->slot[r->slot];
-        const double rstart = r_lo + (double)t->chunks[r->chunk].i0 * lodr;
-        const double rfreq = rstart + (double)r->j * lodr;
-        const double kmul = (double)s->k;
-        const double rsel = kmul != 1.0 ? kmul * rfreq : rfreq;
-        if (r->slot != 0 && !(rsel < nyq)) continue;
-        Candidate cd;
-        cd.freq = rsel / T;
-        cd.metric = metric;
-        cd.r = rsel;
-        cd.nharm = s->Hk;
-        cd.ducy = NAN;
-        candlist_push(out, cd);
-    }
+    Candidate cd;
+    for (i = 0; i < n; i++)
+        if (harvest_one(t, recs[i].chunk, recs[i].slot, recs[i].j, (double)recs[i].metric,
+                        r_lo, lodr, N / 2.0, T, threshold, &cd))
+            candlist_push(out, cd);
+}
+
+static int rec64_cmp(const void *a, const void *b)
+{
+    const CsRec64 *x = (const CsRec64 *)a, *y = (const CsRec64 *)b;
+    if (x->chunk != y->chunk) return (x->chunk > y->chunk) - (x->chunk < y->chunk);
+    if (x->slot != y->slot) return (x->slot > y->slot) - (x->slot < y->slot);
+    return (x->j > y->j) - (x->j < y->j);
+}
+
+/* FP64 searches are rare and their record lists short: a comparison sort
+ * (each (chunk, slot, j) appears once, so the order is total). */
+CS_HIDDEN_API void cs_sort_records64(CsRec64 *recs, long long n)
+{
+    if (n > 1) qsort(recs, (size_t)n, sizeof(CsRec64), rec64_cmp);
+}
+
+CS_HIDDEN_API void cs_harvest64(const CsTables *t, const CsRec64 *recs, long long n,
+                                double r_lo, double lodr, double N, double T,
+                                double threshold, CandidateList *out)
+{
+    long long i;
+    Candidate cd;
+    for (i = 0; i < n; i++)
+        if (harvest_one(t, recs[i].chunk, recs[i].slot, recs[i].j, recs[i].metric,
+                        r_lo, lodr, N / 2.0, T, threshold, &cd))
+            candlist_push(out, cd);
 }

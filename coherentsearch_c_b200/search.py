@@ -36,6 +36,7 @@ class Options:
     harm_remove: bool = True
     boxcar_fsp: float = 1.5
     boxcar_maxfrac: float = 0.3
+    precision: int = 0              # 0: f32, 1: f64 (--precision, CS_PREC_F64)
 
     def params(self, lib) -> nt.SearchParams:
         p = nt.SearchParams()
@@ -47,6 +48,7 @@ class Options:
         p.boxcar_fsp = self.boxcar_fsp
         p.boxcar_maxfrac = self.boxcar_maxfrac
         p.ndecim = lib.decimation_set(self.nharms, self.maxdecim, p.decimations, 64)
+        p.precision = self.precision
         return p
 
     def geometry(self, N: int, dt: float):

@@ -28,7 +28,8 @@ typedef struct {
     long long total;     /* trials */
     unsigned rec_capacity;
     int kernel;          /* 0: generic fused kernel, 1: warp-specialised
-                            kernel for the default nharms = 60 ladder */
+                            kernel for the default ladder (nharms 60, 32,
+                            16), 2: the FP64 search (--precision f64) */
 } CsB200Info;
 
 int cs_b200_session_info(const GpuSession *s, CsB200Info *info);

@@ -70,16 +70,19 @@ def _run(cmd, cwd):
 
 @needs_dropin
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["small", "precision"])
+@pytest.mark.parametrize("case", ["small", "precision", "small_f64", "precision_f64"])
 def test_reference_cli_on_gpu_matches_cpu(gpu_ready, tmp_path, case):
-    if case == "small":
+    """`*_f64` run both sides with --precision f64: the GPU side then takes
+    the FP64 search (the reference's CPU f64 path is the FP64 oracle)."""
+    if case.startswith("small"):
         spec = synth.config_small()
         extra = []
     else:
         spec = synth.config_precision(N=1 << 22)
         extra = ["--threads", str(min(16, os.cpu_count() or 1))]
+    prec = ["--precision", "f64"] if case.endswith("_f64") else []
     dat = _write(str(tmp_path), case, spec)
-    common = ["-t", "8", "--blocksize", "2048"]
+    common = ["-t", "8", "--blocksize", "2048"] + prec
     _run([CPU_BIN] + common + extra + ["-o", "cpu.cohout", dat], str(tmp_path))
     _run([GPU_BIN, "--gpu", "0"] + common + ["-o", "gpu.cohout", dat], str(tmp_path))
     same_cohout(str(tmp_path / "gpu.cohout"), str(tmp_path / "cpu.cohout"))
