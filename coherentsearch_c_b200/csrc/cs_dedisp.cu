@@ -410,6 +410,11 @@ constexpr int FS = 4;           /* samples per thread */
 constexpr int FT = 256 * FS;    /* samples per CTA */
 constexpr int FR = 4;           /* most subbands per round */
 constexpr int FMAXSUB = 256;    /* most subbands (staged offsets) */
+/* Three CTAs of 256 threads per SM leave 85 registers a thread (80 after
+ * allocation granularity); FG x FS sums take 64 of them.  ptxas reports 80
+ * registers with 124 bytes of spill stores at FG 16, FS 4: any larger product
+ * would spill the sums themselves, so it needs the two-CTA bound instead. */
+static_assert(FG * FS <= 64, "dd_dms_f32: the sums must fit the three-CTA register budget");
 
 static __device__ __forceinline__ void cp_async_commit()
 {

@@ -1585,16 +1585,48 @@ constexpr size_t NOALLOC_BYTES = NOALLOC_HDR + (size_t)CS_B200_NOALLOC_MAX_RECS 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
-static unsigned char *g_noalloc_ptr[NOALLOC_MAX_DEVICES];
 
-/* Device address of this device's scratch; looked up once per device with
- * that device current.  The lookup can load the module, so the first call on
- * a device belongs before any stream capture. */
+/* The address is cached per device together with the context it belongs to:
+ * a cudaDeviceReset (or a new primary context) maps the module again, maybe
+ * elsewhere, so a cached address is used only while its context is current.
+ * The context comes from the driver's cuCtxGetCurrent, reached through the
+ * runtime's entry-point query; where that is unavailable the address is
+ * looked up on every call (a symbol lookup, no allocation). */
+struct NoallocSlot {
+    void *ctx;
+    unsigned char *ptr;
+};
+static NoallocSlot g_noalloc_slot[NOALLOC_MAX_DEVICES];
+static std::mutex g_noalloc_mu;
+
+typedef int (*CtxGetCurrentFn)(void **);
+static CtxGetCurrentFn ctx_get_current()
+{
+    static const CtxGetCurrentFn fn = [] {
+        void *p = NULL;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) !=
+                cudaSuccess || q != cudaDriverEntryPointSuccess)
+            p = NULL;
+        return (CtxGetCurrentFn)p;
+    }();
+    return fn;
+}
+
+/* Device address of this device's scratch, for the context current on the
+ * calling thread (the caller has made `device` current).  Looked up with
+ * cudaGetSymbolAddress on the first call in a context; that lookup can load
+ * the module, so the first call on a device belongs before any stream
+ * capture. */
 static unsigned char *noalloc_scratch(int device)
 {
     if (device < 0 || device >= NOALLOC_MAX_DEVICES) return NULL;
-    unsigned char *p = __atomic_load_n(&g_noalloc_ptr[device], __ATOMIC_ACQUIRE);
-    if (p) return p;
+    void *ctx = NULL;
+    const CtxGetCurrentFn get = ctx_get_current();
+    const bool have_ctx = get && get(&ctx) == 0 && ctx;
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    NoallocSlot &sl = g_noalloc_slot[device];
+    if (have_ctx && sl.ptr && sl.ctx == ctx) return sl.ptr;
     void *addr = NULL;
     const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
     if (e != cudaSuccess || !addr) {
@@ -1602,8 +1634,8 @@ static unsigned char *noalloc_scratch(int device)
                 cudaGetErrorString(e));
         return NULL;
     }
-    /* racing first calls store the same address */
-    __atomic_store_n(&g_noalloc_ptr[device], (unsigned char *)addr, __ATOMIC_RELEASE);
+    sl.ctx = have_ctx ? ctx : NULL;
+    sl.ptr = have_ctx ? (unsigned char *)addr : NULL;
     return (unsigned char *)addr;
 }
 
@@ -1678,7 +1710,15 @@ CS_EXPORT int cs_b200_session_search_noalloc(GpuSession *S, const float *d_amps,
     cudaStream_t st = stream ? (cudaStream_t)stream : S->st;
     const float2 *amps = d_amps ? (const float2 *)d_amps : S->d_amps;
 
-    cudaError_t e = cudaMemsetAsync(base, 0, 4 * sizeof(unsigned), st);
+    cudaError_t e = cudaSuccess;
+    if (st != S->st) {
+        /* the caller's stream first waits for what is queued on the session
+         * stream (a spectrum upload into the session buffer, an earlier
+         * search): the hand-off event exists since the session was made */
+        if ((e = cudaEventRecord(S->ev_in, S->st)) == cudaSuccess)
+            e = cudaStreamWaitEvent(st, S->ev_in, 0);
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(base, 0, 4 * sizeof(unsigned), st);
     if (e == cudaSuccess && S->namps > 0) {
         int g = (int)std::min<long long>((S->namps + 255) / 256, (long long)S->nsm * 8);
         cs_amax_kernel<<<g, 256, 0, st>>>(amps, S->namps, amax);

@@ -296,8 +296,9 @@ int cs_b200_session_park_drain(void);
  * nothing, on the device or the host: its per-call scratch (spectrum maximum,
  * record counter, error flag, and up to CS_B200_NOALLOC_MAX_RECS records of
  * 16 bytes, about 1 MiB) is a static device array, cleared at the start of
- * each call.  The first call on a device looks up that array's address and
- * should come before any stream capture.  The scratch is shared by every
+ * each call.  The first call on a device (and the first after a
+ * cudaDeviceReset) looks up that array's address and should come before any
+ * stream capture.  The scratch is shared by every
  * session on a device, so calls that overlap on the GPU (two streams, two
  * host threads) race and must be serialised by the caller.
  *
@@ -305,7 +306,8 @@ int cs_b200_session_park_drain(void);
  * out/cap: caller-owned host array for the candidates; also used as staging
  * for the raw records, so cap must be at least the number of records above
  * the threshold.  stream: a cudaStream_t, or NULL for the session stream; the
- * call waits for it.  The candidates equal those of cs_gpu_session_run in
+ * work runs on it after what is already queued on the session stream, and
+ * the call waits for it.  The candidates equal those of cs_gpu_session_run in
  * content and order.  Returns 0 and *nout, -1 on a CUDA or kernel error, -2
  * when more than CS_B200_NOALLOC_MAX_RECS records pass the threshold (nothing
  * is returned; raise the threshold or use cs_gpu_session_run), -3 when cap is
