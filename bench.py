@@ -460,6 +460,22 @@ def run_b200(args):
                                                              ours=ses.collapse(out))
         except Exception as exc:   # noqa: BLE001
             line["plain_reference_gpu"] = {"unavailable": str(exc)}
+    if rank == 0 and world == 1 and not args.no_extras:
+        # the batched and served forms in short (the sweep and serve workloads
+        # have full lines of their own: --workload sweep / serve)
+        try:
+            lines, _ = sweep_lines(64, args.slots, [60], 1, 1, not args.no_ref_gpu, device=local)
+            line["sweep"] = dict(lines[60], files=64,
+                                 workload="64 spectra, lengths log-uniform 2^21-2^23 (dt 64 us), "
+                                          "pulsar 11.2 Hz peaking mid-list, nharms 60; "
+                                          f"{args.slots} batch slots; P1 = a session per file")
+        except Exception as exc:   # noqa: BLE001
+            line["sweep"] = {"unavailable": str(exc)}
+        try:
+            line["serve"] = serve_summary(400, 200.0, 24, args.slots, args.mem_budget_gb,
+                                          not args.no_ref_gpu)
+        except Exception as exc:   # noqa: BLE001
+            line["serve"] = {"unavailable": str(exc)}
     if rank == 0:
         print(json.dumps(line))
     ses.close()
@@ -903,18 +919,19 @@ def sweep_reference_gpu(specs, spectra, dt, opts, trials, ours, batched_ms):
             "source": "reference src/cuda.cu built for sm_100a, one SearchCache over the list"}
 
 
-def run_sweep(args):
-    """Config 3: 256 files of uneven length searched plain (a session per
-    file, the reference's single-file GPU form) and batched (cs_gpu_batch)."""
+def sweep_lines(files, slots, nh_list, steps, warmup, ref_gpu, device=0):
+    """Config 3 measured: `files` spectra of uneven length searched plain (P1:
+    a session per file, this library's single-file form) and batched
+    (cs_gpu_batch), optionally beside the reference's own GPU form (P0), per
+    harmonic count.  Returns ({nh: summary}, spectra)."""
     import torch
     from coherentsearch_c_b200 import synth
     from coherentsearch_c_b200.batch import Batch
     from coherentsearch_c_b200.search import Options, Session
-    torch.cuda.set_device(0)
-    specs = synth.config_dm_sweep(n_files=args.files)
+    specs = synth.config_dm_sweep(n_files=files)
     dt = specs[0].dt
-    spectra = [spectrum_device(sp.N, dt, sp.seed, sp.pulsars, "cuda:0").numpy() for sp in specs]
-    nh_list = [60, 32]
+    spectra = [spectrum_device(sp.N, dt, sp.seed, sp.pulsars, f"cuda:{device}").numpy()
+               for sp in specs]
     lines = {}
     for nh in nh_list:
         opts = Options(nharms=nh, blocksize=65536, threshold=8.0)
@@ -929,19 +946,19 @@ def run_sweep(args):
             return out
 
         def batched():
-            with Batch(nslots=args.slots) as b:
+            with Batch(nslots=slots) as b:
                 ids = [b.submit(a, sp.N, dt, opts) for sp, a in zip(specs, spectra)]
                 return [b.wait(i)[0] for i in ids]
 
-        for _ in range(args.warmup):      # warm: modules, allocator, page cache
-            with Batch(nslots=args.slots) as b:
+        for _ in range(warmup):           # warm: modules, allocator, page cache
+            with Batch(nslots=slots) as b:
                 for i in [b.submit(a, sp.N, dt, opts) for sp, a in zip(specs[:4], spectra[:4])]:
                     b.wait(i)
         stream = torch.cuda.current_stream()
         res = {}
         for name, fn in (("plain", plain), ("batched", batched)):
             ts = []
-            for _ in range(max(1, min(args.steps, 2))):
+            for _ in range(max(1, min(steps, 2))):
                 torch.cuda.synchronize()
                 e0 = torch.cuda.Event(enable_timing=True)
                 e1 = torch.cuda.Event(enable_timing=True)
@@ -961,9 +978,19 @@ def run_sweep(args):
                      "equal_candidates": bool(equal), "differing_files": diff,
                      "candidates": int(sum(o.size for o in res["batched"][1])),
                      "plain_candidates": int(sum(o.size for o in res["plain"][1]))}
-        if not args.no_ref_gpu:
+        if ref_gpu:
             lines[nh]["plain_reference_gpu"] = sweep_reference_gpu(
                 specs, spectra, dt, opts, trials, res["batched"][1], res["batched"][0])
+    return lines, spectra
+
+
+def run_sweep(args):
+    """Config 3: 256 files of uneven length searched plain (a session per
+    file, the reference's single-file GPU form) and batched (cs_gpu_batch)."""
+    import torch
+    torch.cuda.set_device(0)
+    lines, spectra = sweep_lines(args.files, args.slots, [60, 32], args.steps, args.warmup,
+                                 not args.no_ref_gpu)
     h2d = int(sum(a.nbytes for a in spectra))
     main = lines[60]
     line = {
@@ -985,18 +1012,15 @@ def run_sweep(args):
     return 0
 
 
-def run_serve(args):
-    """Config 5: a Poisson stream of search requests served by the request
-    loop (continuous batching) and by the plain per-request form."""
-    import torch
+def serve_requests(nreq, npool, device=0):
+    """Config 5's requests: a pool of seeded spectra (N log-uniform 2^20-2^24,
+    30 % with a pulsar) and `nreq` requests drawn from it with nharms uniform
+    in {16, 32, 60}."""
     from coherentsearch_c_b200 import synth
     from coherentsearch_c_b200.search import Options
-    from coherentsearch_c_b200.serve import (PlainServer, Request, SearchServer,
-                                             log_uniform_lengths, poisson_arrivals, run_stream)
-    torch.cuda.set_device(0)
+    from coherentsearch_c_b200.serve import Request, log_uniform_lengths
     rng = np.random.default_rng(7)
     dt = 64e-6
-    npool = args.pool
     lengths = log_uniform_lengths(npool, 1 << 20, 1 << 24, seed=11)
     pool = []
     for i, N in enumerate(lengths):
@@ -1004,12 +1028,89 @@ def run_serve(args):
         if rng.random() < 0.3:
             pulsars = [synth.Pulsar(float(math.exp(rng.uniform(math.log(0.5), math.log(100.0)))),
                                     float(rng.uniform(0.02, 0.10)), float(rng.uniform(8, 30)))]
-        pool.append((N, spectrum_device(N, dt, 5000 + i, pulsars, "cuda:0").numpy()))
+        pool.append((N, spectrum_device(N, dt, 5000 + i, pulsars, f"cuda:{device}").numpy()))
     reqs = []
-    for i in range(args.requests):
+    for i in range(nreq):
         N, a = pool[int(rng.integers(npool))]
         nh = int(rng.choice([16, 32, 60]))
         reqs.append(Request(a, N, dt, Options(nharms=nh, blocksize=65536, threshold=8.0)))
+    return reqs, max(lengths)
+
+
+def serve_capacity(reqs, maxlen, slots, budget_gb):
+    """Closed loop: every request submitted at once, served (continuous
+    batching) and plain (a session per request).  The served throughput is
+    the capacity of the engine; p50/p99 are latencies under saturation."""
+    from coherentsearch_c_b200.search import Options
+    from coherentsearch_c_b200.serve import PlainServer, SearchServer, run_stream
+    zero = np.zeros(len(reqs))
+    with SearchServer(nslots=slots, mem_budget=budget_gb << 30) as srv:
+        srv.warm(maxlen, 64e-6, Options(nharms=60, blocksize=65536, threshold=8.0))
+        served = run_stream(srv, reqs, zero)
+    with PlainServer() as pl:
+        plain = run_stream(pl, reqs, zero)
+    return {"requests": len(reqs), "served_trials_per_s": served["trials_per_s"],
+            "served_requests_per_s": len(reqs) / served["wall_s"],
+            "served_p50_ms": served["p50_ms"], "served_p99_ms": served["p99_ms"],
+            "plain_trials_per_s": plain["trials_per_s"],
+            "plain_requests_per_s": len(reqs) / plain["wall_s"],
+            "served_vs_plain": served["trials_per_s"] / plain["trials_per_s"],
+            "equal_candidates": bool(all(_same_cands(x, y) for x, y in
+                                         zip(served["results"], plain["results"])))}
+
+
+def serve_summary(nreq, rate, npool, slots, budget_gb, ref_gpu):
+    """Config 5 in short: an open-loop Poisson stream at `rate` (served and
+    plain, p50/p99 from arrival to result), then the closed-loop capacity of
+    both forms on the same requests, and the reference's own GPU form (P0)
+    back to back on the first requests."""
+    from coherentsearch_c_b200.search import Options
+    from coherentsearch_c_b200.serve import (PlainServer, SearchServer, poisson_arrivals,
+                                             run_stream)
+    reqs, maxlen = serve_requests(nreq, npool)
+    arrivals = poisson_arrivals(len(reqs), rate=rate, seed=3)
+    with SearchServer(nslots=slots) as srv:              # warm both forms
+        run_stream(srv, reqs[:6], np.zeros(6))
+    with PlainServer() as pl:
+        run_stream(pl, reqs[:3], np.zeros(3))
+    with SearchServer(nslots=slots, mem_budget=budget_gb << 30) as srv:
+        srv.warm(maxlen, 64e-6, Options(nharms=60, blocksize=65536, threshold=8.0))
+        served = run_stream(srv, reqs, arrivals)
+    with PlainServer() as pl:
+        plain = run_stream(pl, reqs, arrivals)
+    out = {"workload": f"{len(reqs)} requests, Poisson {rate}/s, N log-uniform 2^20-2^24, "
+                       f"nharms in {{16, 32, 60}}, 30% with a pulsar (pool of {npool}); "
+                       f"{slots} slots",
+           "open_loop": {"served_p50_ms": served["p50_ms"], "served_p99_ms": served["p99_ms"],
+                         "served_trials_per_s": served["trials_per_s"],
+                         "plain_p50_ms": plain["p50_ms"], "plain_p99_ms": plain["p99_ms"],
+                         "plain_trials_per_s": plain["trials_per_s"],
+                         "equal_candidates": bool(all(_same_cands(x, y) for x, y in
+                                                      zip(served["results"],
+                                                          plain["results"])))},
+           "closed_loop": serve_capacity(reqs, maxlen, slots, budget_gb)}
+    if ref_gpu:
+        p0 = serve_reference_gpu(reqs, served["results"], served["trials_per_s"], limit=30)
+        out["plain_reference_gpu"] = p0
+        rate0 = p0.get("trials_per_s") if isinstance(p0, dict) else None
+        if rate0:
+            out["closed_loop"]["served_vs_reference_gpu"] = (
+                out["closed_loop"]["served_trials_per_s"] / rate0)
+    return out
+
+
+def run_serve(args):
+    """Config 5: a Poisson stream of search requests served by the request
+    loop (continuous batching) and by the plain per-request form."""
+    import torch
+    from coherentsearch_c_b200.search import Options
+    from coherentsearch_c_b200.serve import (PlainServer, SearchServer, poisson_arrivals,
+                                             run_stream)
+    torch.cuda.set_device(0)
+    dt = 64e-6
+    npool = args.pool
+    reqs, maxlen = serve_requests(args.requests, npool)
+    lengths = [maxlen]
     arrivals = poisson_arrivals(len(reqs), rate=args.rate, seed=3)
     # warm both forms on a few requests
     with SearchServer(nslots=args.slots) as srv:
@@ -1243,6 +1344,8 @@ def main():
     ap.add_argument("--pool", type=int, default=48, help="serve: distinct spectra")
     ap.add_argument("--mem-budget-gb", type=int, default=24, help="serve: device budget")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="search: skip the short sweep and serve summaries")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip the reference's own GPU form (plain single-file baseline)")
     ap.add_argument("--clipped", action="store_true",
