@@ -55,6 +55,10 @@ DFT_FLOP_PER_TRIAL = 28560.0      # 2*(2nh-1)*2nh at nh=60 (k | nh folds add non
 SIMT_OPS_PER_TRIAL = 6000.0       # interp 1920 FMA + 360 rotate + boxcar/fold ~3700
 
 
+KERNEL_NAMES = {0: "cs_search_kernel", 1: "search_ws_cfg60", 2: "search_f64",
+                3: "search_tma_cfg60"}
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -411,7 +415,7 @@ def run_b200(args):
     f_sm = (clocks.get("sm_mhz") or 1965.0) * 1e6
     simt_peak = 148 * 128 * f_sm
     simt_ach = total * SIMT_OPS_PER_TRIAL / (kms * 1e-3)
-    kname = "search_ws_cfg60" if info.kernel == 1 else "cs_search_kernel"
+    kname = KERNEL_NAMES.get(info.kernel, "unknown")
     traffic = profiled_traffic(kname, total)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -1269,7 +1273,7 @@ def run_series(args):
         "gpu_launches": 16 * args.steps,     # 4 spectrum, 2 search, 10 collapse (cuFFT, CUB not counted)
         "roofline": {"bound": "tensor", "achieved": dft, "peak": tc_peak, "unit": "TFLOP/s",
                      "frac": dft / tc_peak, "traffic": None,
-                     "kernel": "search_ws_cfg60" if ses.info().kernel == 1 else "cs_search_kernel",
+                     "kernel": KERNEL_NAMES.get(ses.info().kernel, "unknown"),
                      "kernel_ms": kms, "peak_kind": f"bf16 dense, {peak_kind}"},
         "candidates": int(out.size),
         "clocks": clk.summary(),

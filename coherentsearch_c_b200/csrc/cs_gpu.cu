@@ -31,6 +31,7 @@
  * limit); on expiry the kernel records an error, frees its tensor memory and
  * returns, and the host reports the failure instead of hanging.
  */
+#include <cuda.h>              /* CUtensorMap and its enums (types only) */
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 
@@ -617,6 +618,7 @@ cs_search_kernel(const SearchArgs args)
 }
 
 #include "cs_search_ws.cuh"
+#include "cs_search_tma.cuh"
 #include "cs_search_f64.cuh"
 #include "cs_collapse.h"
 
@@ -679,6 +681,14 @@ struct GpuSession {
     float4 *d_AC;
     wsk::Harm *d_harm2;
     wsk::Harm hh[wsk::MAX_NH];
+    /* column-tile kernel with TMA-staged windows (search_tma) */
+    int use_tma;
+    float *d_wtab;         /* weights by trial index */
+    int *d_cchunk;         /* chunk of each column tile's first trial */
+    CUtensorMap *d_maps;   /* [nh][2] */
+    float2 *d_tc[2];       /* zero-padded spectrum copies (second shifted a bin) */
+    size_t c_wtab, c_cchunk, c_tc;
+    wsk::TArgs tx;
     /* FP64 search (p->precision == CS_PREC_F64) */
     int prec64;
     f64k::Extra fx;
@@ -756,6 +766,11 @@ static void session_release(GpuSession *S)
     cudaFree(S->d_Wt);
     cudaFree(S->d_AC);
     cudaFree(S->d_harm2);
+    cudaFree(S->d_wtab);
+    cudaFree(S->d_cchunk);
+    cudaFree(S->d_maps);
+    cudaFree(S->d_tc[0]);
+    cudaFree(S->d_tc[1]);
     cudaFree(S->d_bcs);
     cudaFree(S->d_scales);
     cudaFree(S->d_recs64);
@@ -852,6 +867,170 @@ static int ws_config(const CsTables &t, long long total)
     if ((double)t.q * 5.0 * t.q >= 4294967295.0) return 0;
     for (int h = 0; h < t.nh; h++) if (t.harm[h].P > wsk::WT_STRIDE) return 0;
     return t.nh;
+}
+
+static cudaError_t dev_reserve(void **p, size_t *cap, size_t need);
+static uint32_t magic_for(int d);
+
+/* The column-tile kernel takes the search_ws configurations when the trial
+ * grid has period q = 2*nharms (hidr 0.5, pnum 1): column tiles of q trials,
+ * rounds of 8.  Returns the nharms of the configuration, or 0. */
+static int tma_config(const CsTables &t, long long total, long long namps, int ws)
+{
+    if (!ws || getenv("CS_B200_WS_KERNEL") || !getenv("CS_B200_TMA_KERNEL")) return 0;
+    if (t.pnum != 1 || t.q != 2 * t.nh || t.q % 8 != 0 || t.q > 128) return 0;
+    for (int h = 0; h < t.nh; h++) if (t.harm[h].rfloor0 < 0) return 0;
+    /* padded copies and box coordinates (2 floats a bin) in 32-bit ints */
+    const double ncol = std::ceil((double)total / t.q / 32.0) * 32.0;
+    double xmax = 0;
+    for (int h = 0; h < t.nh; h++)
+        xmax = std::max(xmax, (double)t.harm[h].rfloor0 + ncol * (h + 1) + t.q);
+    if (2.0 * (xmax + wsk::TMA_FRONT + wsk::TMA_BACK) >= 2147483000.0) return 0;
+    if (2.0 * ((double)namps + wsk::TMA_FRONT + wsk::TMA_BACK) >= 2147483000.0) return 0;
+    return t.nh;
+}
+
+static int tma_smem(int nh)
+{
+    return nh == 60 ? wsk::tma_smem_bytes<wsk::Cfg60>()
+         : nh == 32 ? wsk::tma_smem_bytes<wsk::Cfg32>()
+                    : wsk::tma_smem_bytes<wsk::Cfg16>();
+}
+
+static cudaError_t tma_prepare(int nh)
+{
+    const void *fn = nh == 60 ? (const void *)wsk::search_tma<wsk::Cfg60>
+                   : nh == 32 ? (const void *)wsk::search_tma<wsk::Cfg32>
+                              : (const void *)wsk::search_tma<wsk::Cfg16>;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem(nh));
+}
+
+static void tma_launch(int nh, int grid, cudaStream_t st, const wsk::Args &w, const wsk::TArgs &x)
+{
+    if (nh == 60)
+        wsk::search_tma<wsk::Cfg60><<<grid, 512, tma_smem(60), st>>>(w, x);
+    else if (nh == 32)
+        wsk::search_tma<wsk::Cfg32><<<grid, 512, tma_smem(32), st>>>(w, x);
+    else
+        wsk::search_tma<wsk::Cfg16><<<grid, 512, tma_smem(16), st>>>(w, x);
+}
+
+/* cuTensorMapEncodeTiled, reached through the runtime (libcsgpu links no
+ * driver library). */
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled()
+{
+    static const EncodeTiledFn fn = [] {
+        void *p = NULL;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+                cudaSuccess || q != cudaDriverEntryPointSuccess)
+            p = NULL;
+        return (EncodeTiledFn)p;
+    }();
+    return fn;
+}
+
+/* The tables of the column-tile kernel; false (with the session left on
+ * search_ws) when any step is refused. */
+static bool tma_load(GpuSession *S, const CsTables &t, long long total)
+{
+    const int nh = t.nh, q = t.q;
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return false;
+    /* weights and phase factors by trial index i of a column tile (phase
+     * i mod P_h: P_h divides q) */
+    std::vector<float> wt((size_t)nh * q * wsk::TMA_WROW, 0.0f);
+    for (int h = 0; h < nh; h++) {
+        const int P = t.harm[h].P, off = t.harm[h].woff;
+        for (int i = 0; i < q; i++) {
+            float *d = &wt[((size_t)h * q + i) * wsk::TMA_WROW];
+            const int row = off + i % P;
+            for (int k = 0; k < wsk::M; k++) d[k] = t.W[(size_t)row * t.m + k];
+            d[16] = t.A[2 * (size_t)row];
+            d[17] = t.A[2 * (size_t)row + 1];
+        }
+    }
+    /* chunk of the first trial of every column tile (whole super-tiles) */
+    const long long ncol = (total + q - 1) / q;
+    const long long nsup = (ncol + 31) / 32;
+    std::vector<int> cc((size_t)(nsup * 32));
+    long long ci = 0;
+    for (long long c = 0; c < nsup * 32; c++) {
+        const long long t0 = c * q;
+        while (ci + 1 < t.nchunks && t.chunks[ci + 1].i0 <= t0) ci++;
+        cc[(size_t)c] = (int)ci;
+    }
+    const size_t nbins = (size_t)S->namps + wsk::TMA_FRONT + wsk::TMA_BACK;
+    bool fresh = false;
+    for (int k = 0; k < 2; k++) {
+        if (!S->d_tc[k] || S->c_tc < nbins * sizeof(float2)) fresh = true;
+    }
+    if (fresh) {
+        for (int k = 0; k < 2; k++) {
+            cudaFree(S->d_tc[k]);
+            S->d_tc[k] = NULL;
+        }
+        S->c_tc = 0;
+        for (int k = 0; k < 2; k++)
+            if (cudaMalloc((void **)&S->d_tc[k], nbins * sizeof(float2)) != cudaSuccess) return false;
+        S->c_tc = nbins * sizeof(float2);
+    }
+    /* the pads are zero; the prep kernel rewrites only the spectrum part */
+    for (int k = 0; k < 2; k++)
+        if (cudaMemsetAsync(S->d_tc[k], 0, S->c_tc, S->st) != cudaSuccess) return false;
+    /* per harmonic and copy: 16 rows of 22 bins, rows 2h bins apart; the
+     * inner extent stops 30h bins short of the copy's end, so the last row of
+     * a box never reads past the allocation (those bins are zero anyway) */
+    std::vector<CUtensorMap> maps((size_t)nh * 2);
+    for (int h = 1; h <= nh; h++) {
+        for (int k = 0; k < 2; k++) {
+            const cuuint64_t gdim[2] = {(cuuint64_t)(2 * (nbins - 30 * (size_t)h)),
+                                        (cuuint64_t)wsk::TMA_ROWS};
+            const cuuint64_t gstr[1] = {(cuuint64_t)(16 * h)};
+            const cuuint32_t box[2] = {2 * wsk::TMA_BOXW, wsk::TMA_ROWS};
+            const cuuint32_t est[2] = {1, 1};
+            if (enc(&maps[(size_t)(h - 1) * 2 + k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                    (void *)S->d_tc[k], gdim, gstr, box, est, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+                fprintf(stderr, "Warning: TMA descriptor for harmonic %d refused; using the "
+                                "register-staged kernel\n", h);
+                return false;
+            }
+        }
+    }
+    if (dev_reserve((void **)&S->d_wtab, &S->c_wtab, wt.size() * sizeof(float)) != cudaSuccess ||
+        cudaMemcpyAsync(S->d_wtab, wt.data(), wt.size() * sizeof(float), cudaMemcpyHostToDevice,
+                        S->st) != cudaSuccess)
+        return false;
+    if (dev_reserve((void **)&S->d_cchunk, &S->c_cchunk, cc.size() * sizeof(int)) != cudaSuccess ||
+        cudaMemcpyAsync(S->d_cchunk, cc.data(), cc.size() * sizeof(int), cudaMemcpyHostToDevice,
+                        S->st) != cudaSuccess)
+        return false;
+    if (!S->d_maps && cudaMalloc((void **)&S->d_maps, sizeof(CUtensorMap) * 2 * wsk::MAX_NH) !=
+                          cudaSuccess)
+        return false;
+    if (cudaMemcpyAsync(S->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap),
+                        cudaMemcpyHostToDevice, S->st) != cudaSuccess)
+        return false;
+    /* the host vectors go when this returns: finish the copies first */
+    if (cudaStreamSynchronize(S->st) != cudaSuccess) return false;
+    wsk::TArgs &x = S->tx;
+    memset(&x, 0, sizeof(x));
+    x.maps = S->d_maps;
+    x.wtab = S->d_wtab;
+    x.cchunk = S->d_cchunk;
+    x.nchunks = (int)t.nchunks;
+    x.total = (int)total;
+    x.q = q;
+    x.qmag = magic_for(q);
+    x.rounds_per_super = q / 8;
+    x.nitems = (int)(nsup * (q / 8));
+    return tma_prepare(nh) == cudaSuccess;
 }
 
 static int ws_smem(int nh)
@@ -1045,6 +1224,9 @@ static int session_load(GpuSession *S, const FFTFile *ft, const SearchParams *p,
         CK(cudaMemcpyAsync(S->d_Wt, wfix.data(), wfix.size() * sizeof(float), cudaMemcpyHostToDevice, S->st));
         CK(ws_prepare(S->use_ws));
     }
+    S->use_tma = tma_config(t, total, S->namps, S->use_ws);
+    if (S->use_tma && (tma_smem(S->use_tma) > S->max_smem || !tma_load(S, t, total)))
+        S->use_tma = 0;
     {
         /* Start with room for 1 in 16 trials per slot; grown on overflow. */
         long long want = (total * t.nslot) / 16 + 4096;
@@ -1073,7 +1255,8 @@ static size_t session_bytes(const GpuSession *S)
 {
     return S->c_amps + S->c_rowtab + S->c_W + S->c_A + S->c_carry + S->c_chunks + S->c_tiles +
            S->c_bimg + (size_t)S->cap * sizeof(CsRec) + sizeof(CsHarm) * CS_MAX_NH +
-           S->c_bcs + S->c_scales + (size_t)S->cap64 * sizeof(CsRec64) +
+           S->c_bcs + S->c_scales + (size_t)S->cap64 * sizeof(CsRec64) + S->c_wtab +
+           S->c_cchunk + 2 * S->c_tc + (S->d_maps ? sizeof(CUtensorMap) * 2 * wsk::MAX_NH : 0) +
            (S->d_Wt ? (size_t)wsk::MAX_NH * 4 * wsk::WT_STRIDE * sizeof(float4) : 0);
 }
 
@@ -1233,7 +1416,11 @@ static cudaError_t enqueue_search(GpuSession *S, const float2 *d_amps, double th
     if ((e = cudaMemsetAsync(S->d_err, 0, sizeof(int), S->st)) != cudaSuccess) return e;
     if (S->namps > 0) {
         int g = (int)std::min<long long>((S->namps + 255) / 256, (long long)S->nsm * 8);
-        cs_amax_kernel<<<g, 256, 0, S->st>>>(d_amps, S->namps, S->d_amax);
+        if (S->use_tma)
+            wsk::tma_prep_kernel<<<g, 256, 0, S->st>>>(d_amps, (int)S->namps, S->d_tc[0],
+                                                       S->d_tc[1], S->d_amax);
+        else
+            cs_amax_kernel<<<g, 256, 0, S->st>>>(d_amps, S->namps, S->d_amax);
     }
     if (S->tab.ntiles <= 0) return cudaGetLastError();
     if (S->prec64) {
@@ -1273,6 +1460,13 @@ static cudaError_t enqueue_search(GpuSession *S, const float2 *d_amps, double th
         w.count = S->d_count;
         w.cap = S->cap;
         w.err = S->d_err;
+        if (S->use_tma) {
+            const int grid = std::min(S->tx.nitems, S->nsm);
+            if (timed) cudaEventRecord(S->ev0, S->st);
+            tma_launch(S->use_tma, grid, S->st, w, S->tx);
+            if (timed) cudaEventRecord(S->ev1, S->st);
+            return cudaGetLastError();
+        }
         const int grid = std::min(S->tab.ntiles, S->nsm);
         if (timed) cudaEventRecord(S->ev0, S->st);
         ws_launch(S->use_ws, grid, S->st, w);
@@ -1456,9 +1650,10 @@ CS_EXPORT int cs_b200_session_info(const GpuSession *S, CsB200Info *info)
     info->nslot = S->tab.nslot;
     info->npad = S->tab.npad;
     info->kpad = S->tab.kpad;
-    info->smem_bytes = S->prec64 ? S->f64_smem : S->use_ws ? ws_smem(S->use_ws) : smem_bytes(S->tab);
-    info->grid = std::min(S->tab.ntiles, S->nsm);
-    info->kernel = S->prec64 ? 2 : S->use_ws ? 1 : 0;
+    info->smem_bytes = S->prec64 ? S->f64_smem : S->use_tma ? tma_smem(S->use_tma)
+                     : S->use_ws ? ws_smem(S->use_ws) : smem_bytes(S->tab);
+    info->grid = S->use_tma ? std::min(S->tx.nitems, S->nsm) : std::min(S->tab.ntiles, S->nsm);
+    info->kernel = S->prec64 ? 2 : S->use_tma ? 3 : S->use_ws ? 1 : 0;
     info->total = S->total;
     info->rec_capacity = S->cap;
     return 0;

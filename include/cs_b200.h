@@ -29,7 +29,9 @@ typedef struct {
     unsigned rec_capacity;
     int kernel;          /* 0: generic fused kernel, 1: warp-specialised
                             kernel for the default ladder (nharms 60, 32,
-                            16), 2: the FP64 search (--precision f64) */
+                            16), 2: the FP64 search (--precision f64),
+                            3: the column-tile kernel with TMA-staged
+                            windows (default ladder, hidr 0.5) */
 } CsB200Info;
 
 int cs_b200_session_info(const GpuSession *s, CsB200Info *info);

@@ -46,19 +46,32 @@ def match_candidates(a, b, thr, rtol):
     return only_a, only_b
 
 
-@pytest.mark.parametrize("nharms,kernel", [(60, "ws"), (32, "ws"), (16, "ws"), (60, "generic"),
+KERNEL_IDS = {"generic": 0, "ws": 1, "tma": 3}
+
+
+def use_kernel(monkeypatch, kernel):
+    """Force one of the FP32 kernels: the column-tile TMA kernel (default for
+    the ladder it covers), the register-staged search_ws, or the generic one."""
+    monkeypatch.delenv("CS_B200_GENERIC_KERNEL", raising=False)
+    monkeypatch.delenv("CS_B200_WS_KERNEL", raising=False)
+    monkeypatch.setenv("CS_B200_TMA_KERNEL", "1")
+    if kernel == "generic":
+        monkeypatch.setenv("CS_B200_GENERIC_KERNEL", "1")
+    elif kernel == "ws":
+        monkeypatch.setenv("CS_B200_WS_KERNEL", "1")
+
+
+@pytest.mark.parametrize("nharms,kernel", [(60, "tma"), (32, "tma"), (16, "tma"), (60, "ws"),
+                                           (32, "ws"), (16, "ws"), (60, "generic"),
                                            (32, "generic"), (16, "generic"), (7, "generic")])
 def test_all_trial_metrics_vs_oracle(gpu_ready, monkeypatch, nharms, kernel):
     """Every trial of every decimation slot: GPU metric vs the oracle's."""
-    if kernel == "generic":
-        monkeypatch.setenv("CS_B200_GENERIC_KERNEL", "1")
-    else:
-        monkeypatch.delenv("CS_B200_GENERIC_KERNEL", raising=False)
+    use_kernel(monkeypatch, kernel)
     spec, amps = _small_case()
     opts = Options(nharms=nharms, blocksize=2048, threshold=-1e30, remove=False,
                    harm_remove=False)
     ses = Session(spec.N, spec.dt, opts)
-    assert ses.info().kernel == (1 if kernel == "ws" else 0)
+    assert ses.info().kernel == KERNEL_IDS[kernel]
     raw = ses.run_raw(amps)
     total = ses.total
     met, geo = rb.oracle_metrics(amps, spec.N, spec.dt, opts, 0, total)
