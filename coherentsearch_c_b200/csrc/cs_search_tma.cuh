@@ -469,7 +469,7 @@ __global__ void tma_prep_kernel(const float2 *__restrict__ amps, int namps,
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < namps; i += gridDim.x * blockDim.x) {
         const float2 v = amps[i];
         c0[TMA_FRONT + i] = v;
-        if (i >= 1) c1[TMA_FRONT + i - 1] = v;
+        c1[TMA_FRONT + i - 1] = v;                  /* TMA_FRONT >= 1 */
         const float m = fmaxf(fabsf(v.x), fabsf(v.y));
         if (!(m <= 3.0e38f)) bad = 1;
         mx = fmaxf(mx, m);
