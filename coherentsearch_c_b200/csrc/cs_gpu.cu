@@ -877,7 +877,7 @@ static uint32_t magic_for(int d);
  * rounds of 8.  Returns the nharms of the configuration, or 0. */
 static int tma_config(const CsTables &t, long long total, long long namps, int ws)
 {
-    if (!ws || getenv("CS_B200_WS_KERNEL")) return 0;
+    if (!ws || getenv("CS_B200_WS_KERNEL") || !getenv("CS_B200_TMA_KERNEL")) return 0;
     if (t.pnum != 1 || t.q != 2 * t.nh || t.q % 8 != 0 || t.q > 128) return 0;
     for (int h = 0; h < t.nh; h++) if (t.harm[h].rfloor0 < 0) return 0;
     /* padded copies and box coordinates (2 floats a bin) in 32-bit ints */

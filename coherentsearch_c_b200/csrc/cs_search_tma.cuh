@@ -56,7 +56,10 @@ constexpr int TMA_WROW = 20;                        /* floats per weight row: 16
 constexpr int TMA_WOFF = 5760;                      /* weight rows of the round */
 constexpr int TMA_WBYTES = 8 * TMA_WROW * 4;        /* 640 */
 constexpr int TMA_STG = 6400;                       /* bytes per stage */
-constexpr int TMA_NSTG = 4;                         /* stages per harmonic set */
+#ifndef WSK_TMA_NSTG
+#define WSK_TMA_NSTG 12
+#endif
+constexpr int TMA_NSTG = WSK_TMA_NSTG;              /* stages per harmonic set */
 constexpr int TMA_TX = 2 * TMA_BOX_BYTES + TMA_WBYTES;
 constexpr int TMA_FRONT = 64;                       /* zero bins before the staged spectrum */
 constexpr int TMA_BACK = 2048;                      /* and after it */
@@ -64,6 +67,9 @@ static_assert(TMA_BOX1 >= TMA_BOX_BYTES && TMA_BOX1 % 128 == 0, "box layout");
 static_assert(TMA_WOFF >= TMA_BOX1 + TMA_BOX_BYTES && TMA_WOFF % 128 == 0, "stage layout");
 static_assert(TMA_WOFF + TMA_WBYTES <= TMA_STG && TMA_STG % 128 == 0, "stage size");
 static_assert(TMA_BACK >= 30 * MAX_NH + 2 * TMA_BOXW, "rows of a box stay inside the copy");
+/* barriers: full[2][NSTG], empty[2][NSTG], a_full, a_empty, d_full, then the
+ * tensor-memory slot */
+constexpr int TMA_BAR_BYTES = (8 * 4 * TMA_NSTG + 24 + 4 + 127) / 128 * 128;
 
 struct TArgs {
     const void *maps;           /* CUtensorMap [nh][2]: copy 0, copy 1 (shifted a bin) */
@@ -173,7 +179,7 @@ static __device__ __forceinline__ void split_hl(float2 x, float scale, uint32_t 
 template <class C>
 __host__ __device__ constexpr int tma_smem_bytes()
 {
-    return 2 * C::NPAD * C::KPAD * 2 + 2 * TMA_NSTG * TMA_STG + 256 + C::NH * (int)sizeof(Harm);
+    return 2 * C::NPAD * C::KPAD * 2 + 2 * TMA_NSTG * TMA_STG + TMA_BAR_BYTES + C::NH * (int)sizeof(Harm);
 }
 
 /* Issue stage n of harmonic set s: the two boxes and the weight rows of
@@ -209,10 +215,7 @@ search_tma(const __grid_constant__ Args a, const __grid_constant__ TArgs x)
     constexpr int HB1 = (NB + 1) / 2;               /* set 0: blocks 0..HB1-1 */
     constexpr int BIMG = NPAD * KPAD * 2;
     constexpr int SM_B = 0, SM_STG = 2 * BIMG, SM_BAR = SM_STG + 2 * TMA_NSTG * TMA_STG;
-    /* barriers: full[2][NSTG], empty[2][NSTG], a_full, a_empty, d_full, then
-     * the tensor-memory slot */
-    constexpr int SM_HARM = SM_BAR + 256;
-    static_assert(8 * 4 * TMA_NSTG + 24 + 4 <= 256, "barrier area");
+    constexpr int SM_HARM = SM_BAR + TMA_BAR_BYTES;
     static_assert(SM_HARM + NH * (int)sizeof(Harm) == tma_smem_bytes<C>(), "layout");
     static_assert(NH % 4 == 0 && 2 * NH <= KPAD && NPAD <= D_STRIDE, "shape");
     extern __shared__ __align__(1024) unsigned char smem[];

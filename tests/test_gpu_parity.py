@@ -54,6 +54,7 @@ def use_kernel(monkeypatch, kernel):
     the ladder it covers), the register-staged search_ws, or the generic one."""
     monkeypatch.delenv("CS_B200_GENERIC_KERNEL", raising=False)
     monkeypatch.delenv("CS_B200_WS_KERNEL", raising=False)
+    monkeypatch.setenv("CS_B200_TMA_KERNEL", "1")
     if kernel == "generic":
         monkeypatch.setenv("CS_B200_GENERIC_KERNEL", "1")
     elif kernel == "ws":
