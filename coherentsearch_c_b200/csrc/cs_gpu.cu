@@ -1766,6 +1766,17 @@ CS_EXPORT int cs_b200_session_sync(GpuSession *S)
     return cudaStreamSynchronize(S->st) == cudaSuccess ? 0 : -1;
 }
 
+#ifdef WSK_TMA_PROF
+/* timing studies only: read and clear the column-tile kernel's counters */
+CS_EXPORT int cs_b200_tma_prof(unsigned long long *out16)
+{
+    if (cudaMemcpyFromSymbol(out16, wsk::g_tma_prof, 16 * sizeof(unsigned long long)) != cudaSuccess)
+        return -1;
+    unsigned long long z[16] = {0};
+    return cudaMemcpyToSymbol(wsk::g_tma_prof, z, sizeof(z)) == cudaSuccess ? 0 : -1;
+}
+#endif
+
 /* ------------------------------------------------------------------ */
 /* Search without allocation (cs_b200_session_search_noalloc)          */
 /* ------------------------------------------------------------------ */

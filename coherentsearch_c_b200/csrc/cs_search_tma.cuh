@@ -71,6 +71,19 @@ static_assert(TMA_BACK >= 30 * MAX_NH + 2 * TMA_BOXW, "rows of a box stay inside
  * tensor-memory slot */
 constexpr int TMA_BAR_BYTES = (8 * 4 * TMA_NSTG + 24 + 4 + 127) / 128 * 128;
 
+/* WSK_TMA_PROF builds (timing studies only) add per-role cycle counters:
+ * 0 interp total, 1 stage-full waits, 2 a_empty waits, 3 refill waits,
+ * 4 epilogue total, 5 d_full waits + barrier, 6 a_full waits (MMA issuer),
+ * 7 epilogue compute. */
+#ifdef WSK_TMA_PROF
+__device__ unsigned long long g_tma_prof[16];
+#define TPROF_T0(v) const long long v = clock64()
+#define TPROF_ADD(i, v) do { if (lane == 0) atomicAdd(&g_tma_prof[i], (unsigned long long)(clock64() - (v))); } while (0)
+#else
+#define TPROF_T0(v)
+#define TPROF_ADD(i, v)
+#endif
+
 struct TArgs {
     const void *maps;           /* CUtensorMap [nh][2]: copy 0, copy 1 (shifted a bin) */
     const float *wtab;          /* [nh][q][TMA_WROW]: weights, A re, A im by trial index */
@@ -130,36 +143,24 @@ static __device__ __forceinline__ void bulk_copy(uint32_t dst, const void *src, 
                  :: "r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
 }
 
-static __device__ __forceinline__ float4 lds128(uint32_t addr)
-{
-    float4 v;
-    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
-                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(addr));
-    return v;
-}
-
-static __device__ __forceinline__ float2 lds64(uint32_t addr)
-{
-    float2 v;
-    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
-    return v;
-}
-
 /* 16-tap FP32 chain (tap order, packed f32x2 FMA: each lane a correctly
- * rounded fma, as two scalar chains) and the unfused rotation. */
+ * rounded fma, as two scalar chains) and the unfused rotation.  wrow points
+ * at a weight row in shared memory: plain loads, so that the compiler can
+ * issue them ahead of the chain (the stage's mbarrier wait, an asm with a
+ * memory clobber, keeps them after the data has landed). */
 template <int OFF>
-static __device__ __forceinline__ float2 chain16(const float2 *v, uint32_t wrow)
+static __device__ __forceinline__ float2 chain16(const float2 *v, const float *wrow)
 {
     float2 acc = make_float2(0.0f, 0.0f);
 #pragma unroll
     for (int i4 = 0; i4 < 4; i4++) {
-        const float4 w = lds128(wrow + 16 * i4);
+        const float4 w = reinterpret_cast<const float4 *>(wrow)[i4];
         acc = __ffma2_rn(make_float2(w.x, w.x), v[OFF + 4 * i4 + 0], acc);
         acc = __ffma2_rn(make_float2(w.y, w.y), v[OFF + 4 * i4 + 1], acc);
         acc = __ffma2_rn(make_float2(w.z, w.z), v[OFF + 4 * i4 + 2], acc);
         acc = __ffma2_rn(make_float2(w.w, w.w), v[OFF + 4 * i4 + 3], acc);
     }
-    const float2 g = lds64(wrow + 64);
+    const float2 g = reinterpret_cast<const float2 *>(wrow)[8];
     return make_float2(__fsub_rn(__fmul_rn(g.x, acc.x), __fmul_rn(g.y, acc.y)),
                        __fadd_rn(__fmul_rn(g.x, acc.y), __fmul_rn(g.y, acc.x)));
 }
@@ -265,6 +266,7 @@ search_tma(const __grid_constant__ Args a, const __grid_constant__ TArgs x)
         const int nseq = nround * nhs;
         const bool leader = (r == 0 && lane == 0);
         const uint32_t stg0 = smem_u32(smem + SM_STG + s * TMA_NSTG * TMA_STG);
+        const unsigned char *stgp0 = smem + SM_STG + s * TMA_NSTG * TMA_STG;
         const uint32_t fullb = bar_full + 8 * TMA_NSTG * s, emptyb = bar_empty + 8 * TMA_NSTG * s;
         const uint32_t tl = (uint32_t)(r * 32) << 16;
         const uint32_t abuf0 = tmem + tl + (uint32_t)TM_A, abuf1 = abuf0 + KPAD;
@@ -287,6 +289,7 @@ search_tma(const __grid_constant__ Args a, const __grid_constant__ TArgs x)
             }
         }
         int n = 0;
+        TPROF_T0(p_all);
         for (int it = 0; it < nround && ok; it++) {
             const int item = item_begin + it;
             const int sup = item / x.rounds_per_super, i0 = 8 * (item % x.rounds_per_super);
@@ -296,10 +299,15 @@ search_tma(const __grid_constant__ Args a, const __grid_constant__ TArgs x)
             unsigned long long fa = 0, fb = 0;
             if (t0 < x.total) fa = a.chunks[chunk_of(a, x, cabs, t0)].filled;
             if (t0 + 1 < x.total) fb = a.chunks[chunk_of(a, x, cabs, t0 + 1)].filled;
-            if (it >= 1 && !mbar_wait(bar_aempty, (it - 1) & 1)) {
-                if (lane == 0) atomicExch(a.err, 1);
-                ok = false;
-                break;
+            {
+                TPROF_T0(p_ae);
+                const bool got = it < 1 || mbar_wait(bar_aempty, (it - 1) & 1);
+                TPROF_ADD(2, p_ae);
+                if (!got) {
+                    if (lane == 0) atomicExch(a.err, 1);
+                    ok = false;
+                    break;
+                }
             }
             tc_fence_after();
             for (int hb = hb0; hb < hb1 && ok; hb++) {
@@ -308,10 +316,14 @@ search_tma(const __grid_constant__ Args a, const __grid_constant__ TArgs x)
                 for (int u = 0; u < 4; u++, n++) {
                     const int h = 4 * hb + u + 1;
                     const int stage = n % TMA_NSTG;
-                    const uint32_t stg = stg0 + stage * TMA_STG;
-                    if (ok && !mbar_wait(fullb + 8 * stage, (n / TMA_NSTG) & 1)) {
-                        if (lane == 0) atomicExch(a.err, 1);
-                        ok = false;
+                    const unsigned char *stgp = stgp0 + stage * TMA_STG;
+                    {
+                        TPROF_T0(p_f);
+                        if (ok && !mbar_wait(fullb + 8 * stage, (n / TMA_NSTG) & 1)) {
+                            if (lane == 0) atomicExch(a.err, 1);
+                            ok = false;
+                        }
+                        TPROF_ADD(1, p_f);
                     }
                     float2 xa = make_float2(0.0f, 0.0f), xb = xa;
                     if (ok) {
@@ -323,17 +335,18 @@ search_tma(const __grid_constant__ Args a, const __grid_constant__ TArgs x)
                         const int ob = roff((uint32_t)(ta + 1), (uint32_t)h, (uint32_t)x.q, x.qmag,
                                             hm.carry_res) - r0;
                         /* 18 bins from the even bin at or below oa (oa <= 3, so in the row) */
-                        const uint32_t rowa = stg + (cls ? TMA_BOX1 : 0) +
-                                              (uint32_t)(row * TMA_BOXW * 8) + (uint32_t)((oa >> 1) * 16);
+                        const float4 *rowa = reinterpret_cast<const float4 *>(
+                            stgp + (cls ? TMA_BOX1 : 0) + row * TMA_BOXW * 8 + (oa >> 1) * 16);
                         float2 v[18];
 #pragma unroll
                         for (int c = 0; c < 9; c++) {
-                            const float4 f = lds128(rowa + 16 * c);
+                            const float4 f = rowa[c];
                             v[2 * c] = make_float2(f.x, f.y);
                             v[2 * c + 1] = make_float2(f.z, f.w);
                         }
-                        const uint32_t wa = stg + TMA_WOFF + (uint32_t)(2 * r * TMA_WROW * 4);
-                        const uint32_t wb = wa + TMA_WROW * 4;
+                        const float *wa = reinterpret_cast<const float *>(stgp + TMA_WOFF) +
+                                          2 * r * TMA_WROW;
+                        const float *wb = wa + TMA_WROW;
                         const int pa = oa & 1, db = ob - oa;
                         if (pa == 0) {
                             xa = chain16<0>(v, wa);
@@ -351,7 +364,14 @@ search_tma(const __grid_constant__ Args a, const __grid_constant__ TArgs x)
                      * or nearly) with step n-1+NSTG */
                     if (leader && ok && n >= 1 && issued < nseq && issued == n - 1 + TMA_NSTG) {
                         const int ps = (n - 1) % TMA_NSTG;
+#ifdef WSK_TMA_PROF
+                        const long long p_r = clock64();
+                        const bool got_e = mbar_wait(emptyb + 8 * ps, ((n - 1) / TMA_NSTG) & 1);
+                        atomicAdd(&g_tma_prof[3], (unsigned long long)(clock64() - p_r));
+                        if (!got_e) {
+#else
                         if (!mbar_wait(emptyb + 8 * ps, ((n - 1) / TMA_NSTG) & 1)) {
+#endif
                             atomicExch(a.err, 1);
                             ok = false;
                         } else {
@@ -374,6 +394,7 @@ search_tma(const __grid_constant__ Args a, const __grid_constant__ TArgs x)
             __syncwarp();
             if (lane == 0) mbar_arrive(bar_afull);
         }
+        TPROF_ADD(0, p_all);
         if (!ok && lane == 0) atomicExch(a.err, 1);
         /* drain: every stage this set issued has landed before the CTA ends */
         if (leader) {
@@ -392,9 +413,17 @@ search_tma(const __grid_constant__ Args a, const __grid_constant__ TArgs x)
         const int col = col_of_lane(lane);
         int issued = 0, consumed = 0;
         bool ok = true;
+        TPROF_T0(p_all);
         for (int it = 0; it < nround; it++) {
             if (leader && ok) {
+#ifdef WSK_TMA_PROF
+                const long long p_a = clock64();
+                const bool got_a = mbar_wait(bar_afull, it & 1);
+                atomicAdd(&g_tma_prof[6], (unsigned long long)(clock64() - p_a));
+                if (!got_a) {
+#else
                 if (!mbar_wait(bar_afull, it & 1)) {
+#endif
                     ok = false;
                     atomicExch(a.err, 1);
                 } else {
@@ -423,12 +452,16 @@ search_tma(const __grid_constant__ Args a, const __grid_constant__ TArgs x)
                 }
             }
             __syncwarp();
+            TPROF_T0(p_d);
             const bool got = mbar_wait(bar_dfull, it & 1);
-            if (!epi_bar_and(got && ok)) {
+            const bool all = epi_bar_and(got && ok);
+            TPROF_ADD(5, p_d);
+            if (!all) {
                 if (lane == 0) atomicExch(a.err, 1);
                 ok = false;
                 break;
             }
+            TPROF_T0(p_e);
             consumed++;
             tc_fence_after();
             const int item = item_begin + it;
@@ -445,9 +478,11 @@ search_tma(const __grid_constant__ Args a, const __grid_constant__ TArgs x)
                                       ((uint32_t)(quarter * 32) << 16);
                 C::epilogue(grp, trow, ch, a, valid, ci, j, lane, inv_scale);
             }
+            TPROF_ADD(7, p_e);
             tc_fence_before();
             epi_bar_and(true);      /* D0 and D1 free for the MMAs of the next round */
         }
+        TPROF_ADD(4, p_all);
         /* drain: never free tensor memory under an MMA in flight */
         if (leader) {
             for (int k = consumed; k < issued; k++) mbar_wait(bar_dfull, k & 1);
