@@ -925,17 +925,31 @@ def sweep_reference_gpu(specs, spectra, dt, opts, trials, ours, batched_ms):
 
 def sweep_lines(files, slots, nh_list, steps, warmup, ref_gpu, device=0):
     """Config 3 measured: `files` spectra of uneven length searched plain (P1:
-    a session per file, this library's single-file form) and batched
-    (cs_gpu_batch), optionally beside the reference's own GPU form (P0), per
-    harmonic count.  Returns ({nh: summary}, spectra)."""
+    a session per file, this library's single-file form), batched
+    (cs_gpu_batch: slots, one launch per file) and grouped (sweep.search_list:
+    one persistent launch per group of files, group size from the autotuner
+    on the first 64 files), optionally beside the reference's own GPU form
+    (P0), per harmonic count.  Returns ({nh: summary}, spectra)."""
     import torch
     from coherentsearch_c_b200 import synth
     from coherentsearch_c_b200.batch import Batch
     from coherentsearch_c_b200.search import Options, Session
+    from coherentsearch_c_b200.sweep import autotune, search_list, warm
     specs = synth.config_dm_sweep(n_files=files)
     dt = specs[0].dt
-    spectra = [spectrum_device(sp.N, dt, sp.seed, sp.pulsars, f"cuda:{device}").numpy()
-               for sp in specs]
+    pinned = [spectrum_device(sp.N, dt, sp.seed, sp.pulsars, f"cuda:{device}") for sp in specs]
+    spectra = [p.numpy() for p in pinned]
+    listed = [(sp.N, None) for sp in specs]
+    # device buffers of the grouped form, allocated before any timing; the
+    # copies into them run inside the timed region
+    dev_bufs = [torch.empty(p.numel(), dtype=torch.float32, device=f"cuda:{device}")
+                for p in pinned]
+
+    def upload(i):
+        """Spectrum i to the device on the current stream (pinned source, so
+        the copy overlaps the previous group's kernel)."""
+        dev_bufs[i].copy_(pinned[i], non_blocking=True)
+        return dev_bufs[i].data_ptr()
     lines = {}
     for nh in nh_list:
         opts = Options(nharms=nh, blocksize=65536, threshold=8.0)
@@ -954,13 +968,22 @@ def sweep_lines(files, slots, nh_list, steps, warmup, ref_gpu, device=0):
                 ids = [b.submit(a, sp.N, dt, opts) for sp, a in zip(specs, spectra)]
                 return [b.wait(i)[0] for i in ids]
 
+        st = torch.cuda.current_stream().cuda_stream
+        warm(max(sp.N for sp in specs), dt, opts, 64, device)   # two groups of up to 32
+        group, tune = autotune(listed, dt, opts, candidates=(1, 2, 4, 8, 16, 32), sample=64,
+                               device=device, upload=upload, stream=st,
+                               sync=torch.cuda.synchronize)
+
+        def grouped():
+            return search_list(listed, dt, opts, group, device, upload, st)
+
         for _ in range(warmup):           # warm: modules, allocator, page cache
             with Batch(nslots=slots) as b:
                 for i in [b.submit(a, sp.N, dt, opts) for sp, a in zip(specs[:4], spectra[:4])]:
                     b.wait(i)
         stream = torch.cuda.current_stream()
         res = {}
-        for name, fn in (("plain", plain), ("batched", batched)):
+        for name, fn in (("plain", plain), ("batched", batched), ("grouped", grouped)):
             ts = []
             for _ in range(max(1, min(steps, 2))):
                 torch.cuda.synchronize()
@@ -979,6 +1002,13 @@ def sweep_lines(files, slots, nh_list, steps, warmup, ref_gpu, device=0):
                      "plain_trials_per_s": trials / (res["plain"][0] * 1e-3),
                      "batched_trials_per_s": trials / (res["batched"][0] * 1e-3),
                      "batched_vs_plain": res["plain"][0] / res["batched"][0],
+                     "grouped_ms": res["grouped"][0],
+                     "grouped_trials_per_s": trials / (res["grouped"][0] * 1e-3),
+                     "grouped_vs_plain": res["plain"][0] / res["grouped"][0],
+                     "grouped_files_per_launch": group,
+                     "autotune_seconds_by_group": {str(k): v for k, v in tune.items()},
+                     "grouped_equal_candidates": bool(all(
+                         _same_cands(x, y) for x, y in zip(res["grouped"][1], res["plain"][1]))),
                      "equal_candidates": bool(equal), "differing_files": diff,
                      "candidates": int(sum(o.size for o in res["batched"][1])),
                      "plain_candidates": int(sum(o.size for o in res["plain"][1]))}
@@ -1326,6 +1356,9 @@ def profiled_traffic(kernel, total):
 
 
 def main():
+    # the grouped sweep keeps two groups of sessions (up to 2 x 32) in the
+    # library's session park between groups
+    os.environ.setdefault("CS_B200_SESSION_PARK", "80")
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)

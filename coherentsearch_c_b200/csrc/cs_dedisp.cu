@@ -1053,8 +1053,10 @@ CS_EXPORT int cs_dedisp_last_times(CsDedisp *D, float *subband_ms, float *dm_ms)
     if (cudaEventSynchronize(D->ev2) != cudaSuccess) return -1;
     float a = 0.0f, b = 0.0f;
     if (cudaEventElapsedTime(&a, D->ev0, D->ev1) != cudaSuccess ||
-        cudaEventElapsedTime(&b, D->ev1, D->ev2) != cudaSuccess)
+        cudaEventElapsedTime(&b, D->ev1, D->ev2) != cudaSuccess) {
+        (void)cudaGetLastError();       /* unrecorded events: no stale error left behind */
         return -1;
+    }
     if (subband_ms) *subband_ms = a;
     if (dm_ms) *dm_ms = b;
     return 0;

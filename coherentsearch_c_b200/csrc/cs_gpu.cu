@@ -55,6 +55,9 @@
 
 #define CS_NTHREADS 256
 #define CS_WAIT_NS 2000000000ull  /* 2 s bound on any in-kernel wait */
+#ifndef CS_MBAR_SLEEP_NS
+#define CS_MBAR_SLEEP_NS 64       /* back-off between polls of an mbarrier */
+#endif
 
 /* ------------------------------------------------------------------ */
 /* Kernel arguments                                                   */
@@ -124,7 +127,9 @@ static __device__ bool mbar_wait(uint32_t bar, uint32_t parity)
     const unsigned long long t0 = global_ns();
     while (!mbar_try(bar, parity)) {
         if (global_ns() - t0 > CS_WAIT_NS) return false;
-        __nanosleep(64);     /* leave the issue slots to the working warps */
+#if CS_MBAR_SLEEP_NS > 0
+        __nanosleep(CS_MBAR_SLEEP_NS);   /* leave the issue slots to the working warps */
+#endif
     }
     return true;
 }
@@ -1040,8 +1045,18 @@ static int ws_smem(int nh)
                     : wsk::smem_bytes<wsk::Cfg16>();
 }
 
+static cudaError_t ws_prepare_multi(int nh)
+{
+    const void *fn = nh == 60 ? (const void *)wsk::search_ws_multi<wsk::Cfg60>
+                   : nh == 32 ? (const void *)wsk::search_ws_multi<wsk::Cfg32>
+                              : (const void *)wsk::search_ws_multi<wsk::Cfg16>;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, ws_smem(nh));
+}
+
 static cudaError_t ws_prepare(int nh)
 {
+    const cudaError_t e = ws_prepare_multi(nh);
+    if (e != cudaSuccess) return e;
     const void *fn = nh == 60 ? (const void *)wsk::search_ws<wsk::Cfg60>
                    : nh == 32 ? (const void *)wsk::search_ws<wsk::Cfg32>
                               : (const void *)wsk::search_ws<wsk::Cfg16>;
@@ -1406,6 +1421,33 @@ static SearchArgs make_args(GpuSession *S, const float2 *d_amps, double threshol
     return a;
 }
 
+/* Arguments of the warp-specialised kernels for session S. */
+static wsk::Args ws_args(const GpuSession *S, const float2 *d_amps, double threshold)
+{
+    wsk::Args w;
+    memset(&w, 0, sizeof(w));
+    w.amps = d_amps;
+    w.namps = (int)S->namps;
+    w.Wt = S->d_Wt;
+    w.A = S->d_A;
+    w.harm = S->d_harm2;
+    w.chunks = S->d_chunks;
+    w.tiles = S->d_tiles;
+    w.ntiles = S->tab.ntiles;
+    w.bimg = S->d_bimg;
+    w.q = S->tab.q;
+    w.pnum = S->tab.pnum;
+    w.qmagic = magic_for(S->tab.q);
+    w.gbound = S->tab.gbound;
+    w.amax = S->d_amax;
+    w.thresh = threshold;
+    w.recs = S->d_recs;
+    w.count = S->d_count;
+    w.cap = S->cap;
+    w.err = S->d_err;
+    return w;
+}
+
 /* Enqueue the search of the spectrum at d_amps on S->st (no host sync). */
 static cudaError_t enqueue_search(GpuSession *S, const float2 *d_amps, double threshold,
                                   bool timed)
@@ -1439,27 +1481,7 @@ static cudaError_t enqueue_search(GpuSession *S, const float2 *d_amps, double th
         return cudaGetLastError();
     }
     if (S->use_ws) {
-        wsk::Args w;
-        memset(&w, 0, sizeof(w));
-        w.amps = d_amps;
-        w.namps = (int)S->namps;
-        w.Wt = S->d_Wt;
-        w.A = S->d_A;
-        w.harm = S->d_harm2;
-        w.chunks = S->d_chunks;
-        w.tiles = S->d_tiles;
-        w.ntiles = S->tab.ntiles;
-        w.bimg = S->d_bimg;
-        w.q = S->tab.q;
-        w.pnum = S->tab.pnum;
-        w.qmagic = magic_for(S->tab.q);
-        w.gbound = S->tab.gbound;
-        w.amax = S->d_amax;
-        w.thresh = threshold;
-        w.recs = S->d_recs;
-        w.count = S->d_count;
-        w.cap = S->cap;
-        w.err = S->d_err;
+        const wsk::Args w = ws_args(S, d_amps, threshold);
         if (S->use_tma) {
             const int grid = std::min(S->tx.nitems, S->nsm);
             if (timed) cudaEventRecord(S->ev0, S->st);
@@ -1674,6 +1696,21 @@ CS_EXPORT int cs_b200_session_enqueue_device(GpuSession *S, const float *d_amps,
     return e == cudaSuccess ? 0 : -1;
 }
 
+/* Kernel time of the session's last timed launch, or 0 when its events were
+ * not recorded (a search queued without timing, or one that ran inside a
+ * multi-spectrum launch timed on another session).  The runtime answers an
+ * unrecorded event with an error; it is cleared here so that it does not
+ * surface at the next launch check. */
+static float last_kernel_ms(const GpuSession *S)
+{
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, S->ev0, S->ev1) != cudaSuccess) {
+        (void)cudaGetLastError();
+        ms = 0.0f;
+    }
+    return ms;
+}
+
 CS_EXPORT int cs_b200_session_collect(GpuSession *S, double threshold, CandidateList *out,
                                       float *kernel_ms)
 {
@@ -1681,11 +1718,7 @@ CS_EXPORT int cs_b200_session_collect(GpuSession *S, double threshold, Candidate
     candlist_init(out);
     int rerun = 0;
     if (collect(S, threshold, out, &rerun) != 0) return -1;
-    if (kernel_ms) {
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, S->ev0, S->ev1);
-        *kernel_ms = ms;
-    }
+    if (kernel_ms) *kernel_ms = last_kernel_ms(S);
     return rerun ? 1 : 0;
 }
 
@@ -1733,11 +1766,7 @@ CS_EXPORT int cs_b200_session_collapse_wait(GpuSession *S, CandidateList *out, f
 {
     if (!S || !out) return -1;
     candlist_init(out);
-    if (kernel_ms) {
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, S->ev0, S->ev1);
-        *kernel_ms = ms;
-    }
+    if (kernel_ms) *kernel_ms = last_kernel_ms(S);
     if (!S->coll) return 0;
     return cs_collapse_finish(S->coll, S->st, out) == 0 ? 0 : -1;
 }
@@ -1764,6 +1793,124 @@ CS_EXPORT int cs_b200_session_sync(GpuSession *S)
 {
     if (!S) return -1;
     return cudaStreamSynchronize(S->st) == cudaSuccess ? 0 : -1;
+}
+
+/* ------------------------------------------------------------------ */
+/* Several spectra in one launch (cs_b200_multi_enqueue)               */
+/* ------------------------------------------------------------------ */
+/* Per device: the launch's argument table and tile offsets (grow-only), and
+ * an event marking the last launch that read them. */
+struct MultiTables {
+    wsk::Args *d_files;
+    int *d_off;
+    size_t cap;
+    cudaEvent_t done;
+};
+static std::mutex g_multi_mu;
+static MultiTables g_multi[64];
+
+static cudaError_t multi_launch(int nh, int grid, cudaStream_t st, const wsk::Args &a0,
+                                const wsk::Multi &mu)
+{
+    const void *fn = nh == 60 ? (const void *)wsk::search_ws_multi<wsk::Cfg60>
+                   : nh == 32 ? (const void *)wsk::search_ws_multi<wsk::Cfg32>
+                              : (const void *)wsk::search_ws_multi<wsk::Cfg16>;
+    const int nthr = nh == 60 ? wsk::nthreads<wsk::Cfg60>()
+                   : nh == 32 ? wsk::nthreads<wsk::Cfg32>() : wsk::nthreads<wsk::Cfg16>();
+    wsk::Args a = a0;
+    wsk::Multi m = mu;
+    void *args[2] = {&a, &m};
+    return cudaLaunchKernel(fn, dim3(grid), dim3(nthr), args, (size_t)ws_smem(nh), st);
+}
+
+CS_EXPORT int cs_b200_multi_enqueue(GpuSession **ss, int n, const float *const *d_amps,
+                                    double threshold, void *stream)
+{
+#define MCK(call)                                                                 \
+    do {                                                                          \
+        const cudaError_t e_ = (call);                                            \
+        if (e_ != cudaSuccess) {                                                  \
+            fprintf(stderr, "Error: multi-spectrum launch: %s failed: %s (line %d)\n", \
+                    #call, cudaGetErrorString(e_), __LINE__);                     \
+            return -1;                                                            \
+        }                                                                         \
+    } while (0)
+    if (!ss || n < 1) return -1;
+    GpuSession *S0 = ss[0];
+    for (int i = 0; i < n; i++) {
+        const GpuSession *S = ss[i];
+        if (!S || S->device != S0->device || S->prec64 || !S->use_ws || S->use_ws != S0->use_ws ||
+            S->tab.nslot != S0->tab.nslot || S->tab.npad != S0->tab.npad ||
+            S->tab.kpad != S0->tab.kpad ||
+            memcmp(S->tab.slot, S0->tab.slot, sizeof(CsSlot) * (size_t)S0->tab.nslot) != 0) {
+            fprintf(stderr, "Error: a multi-spectrum launch takes FP32 sessions of one "
+                            "warp-specialised configuration (same nharms and ladder)\n");
+            return -1;
+        }
+    }
+    const int dev = S0->device;
+    if (dev < 0 || dev >= 64) return -1;
+    MCK(select_device(dev));
+    cudaStream_t st = stream ? (cudaStream_t)stream : S0->st;
+    std::lock_guard<std::mutex> g(g_multi_mu);
+    MultiTables &M = g_multi[dev];
+    if (!M.done) MCK(cudaEventCreateWithFlags(&M.done, cudaEventDisableTiming));
+    std::vector<wsk::Args> files((size_t)n);
+    std::vector<int> off((size_t)n + 1, 0);
+    for (int i = 0; i < n; i++) {
+        GpuSession *S = ss[i];
+        /* the launch stream first waits for each session's queued work */
+        if (st != S->st) {
+            MCK(cudaEventRecord(S->ev_in, S->st));
+            MCK(cudaStreamWaitEvent(st, S->ev_in, 0));
+        }
+        const float2 *amps = d_amps && d_amps[i] ? (const float2 *)d_amps[i] : S->d_amps;
+        MCK(cudaMemsetAsync(S->d_amax, 0, 2 * sizeof(unsigned), st));
+        MCK(cudaMemsetAsync(S->d_count, 0, sizeof(unsigned), st));
+        MCK(cudaMemsetAsync(S->d_err, 0, sizeof(int), st));
+        if (S->namps > 0) {
+            const int gr = (int)std::min<long long>((S->namps + 255) / 256, (long long)S->nsm * 8);
+            cs_amax_kernel<<<gr, 256, 0, st>>>(amps, S->namps, S->d_amax);
+            MCK(cudaGetLastError());
+        }
+        files[(size_t)i] = ws_args(S, amps, threshold);
+        off[(size_t)i + 1] = off[(size_t)i] + S->tab.ntiles;
+    }
+    const int ntiles = off[(size_t)n];
+    if (ntiles <= 0) return 0;
+    /* the previous launch on this device may still read the tables */
+    MCK(cudaStreamWaitEvent(st, M.done, 0));
+    if ((size_t)n > M.cap) {
+        MCK(cudaStreamSynchronize(st));
+        cudaFree(M.d_files);
+        cudaFree(M.d_off);
+        M.d_files = NULL;
+        M.d_off = NULL;
+        M.cap = 0;
+        const size_t cap = (size_t)n + 16;
+        MCK(cudaMalloc((void **)&M.d_files, cap * sizeof(wsk::Args)));
+        MCK(cudaMalloc((void **)&M.d_off, (cap + 1) * sizeof(int)));
+        M.cap = cap;
+    }
+    /* pageable sources: each copy returns once its data is staged */
+    MCK(cudaMemcpyAsync(M.d_files, files.data(), files.size() * sizeof(wsk::Args),
+                        cudaMemcpyHostToDevice, st));
+    MCK(cudaMemcpyAsync(M.d_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    wsk::Multi mu;
+    mu.files = M.d_files;
+    mu.tile_off = M.d_off;
+    mu.nfiles = n;
+    mu.ntiles = ntiles;
+    const int grid = std::min(ntiles, S0->nsm);
+    MCK(cudaEventRecord(S0->ev0, st));
+    MCK(multi_launch(S0->use_ws, grid, st, files[0], mu));
+    MCK(cudaEventRecord(S0->ev1, st));
+    MCK(cudaEventRecord(M.done, st));
+    /* each session's later work (its collect) follows the launch */
+    for (int i = 0; i < n; i++)
+        if (ss[i]->st != st) MCK(cudaStreamWaitEvent(ss[i]->st, M.done, 0));
+    return 0;
+#undef MCK
 }
 
 #ifdef WSK_TMA_PROF

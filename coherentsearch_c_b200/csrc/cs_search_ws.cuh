@@ -582,8 +582,49 @@ __host__ __device__ constexpr int smem_bytes()
     return 2 * C::NPAD * C::KPAD * 2 + 64 + 16 + C::NH * (int)sizeof(Harm);
 }
 
-template <class C>
-__global__ void __launch_bounds__(nthreads<C>(), 1) search_ws(const __grid_constant__ Args a)
+/* Several spectra of the same configuration in one persistent launch: a
+ * device table of per-spectrum arguments and the prefix sums of their tile
+ * counts.  Each tile finds its spectrum (binary search) and takes that
+ * spectrum's tables, operand scale and record buffer. */
+struct Multi {
+    const Args *files;
+    const int *tile_off;        /* nfiles + 1 */
+    int nfiles;
+    int ntiles;
+};
+
+/* The arguments and local tile index of global tile g. */
+template <bool MULTI>
+static __device__ __forceinline__ const Args &file_of(const Args &a0, const Multi &mu, int g,
+                                                      int &tile)
+{
+    if (!MULTI) {
+        tile = g;
+        return a0;
+    }
+    int lo = 0, hi = mu.nfiles - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(mu.tile_off + mid) <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    tile = g - __ldg(mu.tile_off + lo);
+    return mu.files[lo];
+}
+
+/* A failed wait: every spectrum of the launch reports the error. */
+template <bool MULTI>
+static __device__ __forceinline__ void set_err(const Args &a0, const Multi &mu)
+{
+    if (!MULTI) {
+        atomicExch(a0.err, 1);
+        return;
+    }
+    for (int f = 0; f < mu.nfiles; f++) atomicExch(mu.files[f].err, 1);
+}
+
+template <class C, bool MULTI>
+static __device__ __forceinline__ void ws_body(const Args &a0, const Multi &mu)
 {
     constexpr int NH = C::NH, NPAD = C::NPAD, KPAD = C::KPAD, AHALF = KPAD / 2;
     constexpr int NIW = C::NIW, NPAR = NIW / 4, NTHREADS = nthreads<C>();
@@ -605,7 +646,8 @@ __global__ void __launch_bounds__(nthreads<C>(), 1) search_ws(const __grid_const
     Harm *hs = reinterpret_cast<Harm *>(smem + SM_HARM);
 
     if (warp == 0) tmem_alloc(smem_u32(tm_slot), TMEM_COLS);
-    for (int h = tid; h < NH; h += NTHREADS) hs[h] = a.harm[h];
+    if (!MULTI)
+        for (int h = tid; h < NH; h += NTHREADS) hs[h] = a0.harm[h];
     if (tid == 0) {
         mbar_init(bar_afull, NIW + 8);      /* every interpolation and epilogue warp */
         mbar_init(bar_afull + 8, NIW + 8);
@@ -616,20 +658,21 @@ __global__ void __launch_bounds__(nthreads<C>(), 1) search_ws(const __grid_const
     }
     {
         uint4 *dst = reinterpret_cast<uint4 *>(smem + SM_B);
-        for (int i = tid; i < (2 * BIMG) / 16; i += NTHREADS) dst[i] = a.bimg[i];
+        for (int i = tid; i < (2 * BIMG) / 16; i += NTHREADS) dst[i] = a0.bimg[i];
     }
     fence_proxy_async();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tm_slot;
-    const float scale = operand_scale(a.amax, a.gbound);
-    const float inv_scale = 1.0f / scale;
+    /* the fp16 operand scale of a spectrum (one per launch unless MULTI) */
+    const float scale0 = MULTI ? 1.0f : operand_scale(a0.amax, a0.gbound);
     /* each CTA owns a contiguous run of tiles: neighbouring tiles read the
      * same spectral windows and weight rows, which then stay in L1 */
-    const int per_cta = (a.ntiles + gridDim.x - 1) / gridDim.x;
-    const int tile_begin = min(a.ntiles, (int)blockIdx.x * per_cta);
-    const int tile_end = min(a.ntiles, tile_begin + per_cta);
+    const int ntiles = MULTI ? mu.ntiles : a0.ntiles;
+    const int per_cta = (ntiles + gridDim.x - 1) / gridDim.x;
+    const int tile_begin = min(ntiles, (int)blockIdx.x * per_cta);
+    const int tile_end = min(ntiles, tile_begin + per_cta);
 
     if (warp < NIW) {
         /* --------------- interpolation of blocks 0..HEAD-1 --------------- */
@@ -649,20 +692,24 @@ __global__ void __launch_bounds__(nthreads<C>(), 1) search_ws(const __grid_const
             }
         }
         int it = 0;
-        for (int tile = tile_begin; tile < tile_end; tile++, it++) {
+        for (int g = tile_begin; g < tile_end; g++, it++) {
             const int s = it & 1;
             if (it >= 2 && !mbar_wait(bar_aempty + 8 * s, ((it - 2) >> 1) & 1)) {
-                if (lane == 0) atomicExch(a.err, 1);
+                if (lane == 0) set_err<MULTI>(a0, mu);
                 break;
             }
             tc_fence_after();
+            int tile;
+            const Args &a = file_of<MULTI>(a0, mu, g, tile);
+            const Harm *hsp = MULTI ? a.harm : hs;
+            const float scale = MULTI ? operand_scale(a.amax, a.gbound) : scale0;
             const TrialState ts = trial_state(a, tile, r);
             const uint32_t abuf = tmem + tlane + (uint32_t)(TM_A + KPAD * s);
             uint32_t res, qint, r4, q4;
             state_at(a, ts, 4u * par + 1u, res, qint);
             state_at(a, ts, 4u * (NPAR - 1), r4, q4);   /* the harmonics other groups take */
             for (int hb = par; hb < HEAD; hb += NPAR) {
-                interp_block<AHALF>(a, hs, ts, hb, res, qint, scale, abuf);
+                interp_block<AHALF>(a, hsp, ts, hb, res, qint, scale, abuf);
                 res += r4; qint += q4;       /* 4hb+5 -> 4(hb+NPAR)+1 */
                 if (res >= (uint32_t)a.q) { res -= (uint32_t)a.q; qint += 1; }
             }
@@ -688,13 +735,17 @@ __global__ void __launch_bounds__(nthreads<C>(), 1) search_ws(const __grid_const
         int issued = 0, consumed = 0;
         bool ok = true;
 
-        auto tail = [&](int it, int tile) {
+        auto tail = [&](int it, int g) {
+            int tile;
+            const Args &a = file_of<MULTI>(a0, mu, g, tile);
+            const Harm *hsp = MULTI ? a.harm : hs;
+            const float scale = MULTI ? operand_scale(a.amax, a.gbound) : scale0;
             const TrialState ts = trial_state(a, tile, r);
             const uint32_t abuf = tmem + tlane + (uint32_t)(TM_A + KPAD * (it & 1));
             uint32_t res, qint;
             state_at(a, ts, 4u * tb0 + 1u, res, qint);
             for (int hb = tb0; hb < tb1; hb++)
-                interp_block<AHALF>(a, hs, ts, hb, res, qint, scale, abuf);
+                interp_block<AHALF>(a, hsp, ts, hb, res, qint, scale, abuf);
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             tc_fence_before();
             __syncwarp();
@@ -729,32 +780,35 @@ __global__ void __launch_bounds__(nthreads<C>(), 1) search_ws(const __grid_const
             if (leader) {
                 ok = issue(0);
                 if (ok) issued = 1;
-                else atomicExch(a.err, 1);
+                else set_err<MULTI>(a0, mu);
             }
             __syncwarp();
         }
         int it = 0;
-        for (int tile = tile_begin; tile < tile_end; tile++, it++) {
+        for (int g = tile_begin; g < tile_end; g++, it++) {
             const int s = it & 1;
-            if (tile + 1 < tile_end) {
+            if (g + 1 < tile_end) {
                 /* A buffer (it+1)&1 was last read by the MMA of tile it-1, whose
                  * accumulator this group already consumed: it is free */
-                tail(it + 1, tile + 1);
+                tail(it + 1, g + 1);
                 if (leader && ok) {
                     ok = issue(it + 1);
                     if (ok) issued++;
-                    else atomicExch(a.err, 1);
+                    else set_err<MULTI>(a0, mu);
                 }
                 __syncwarp();
             }
             bool got = mbar_wait(bar_dfull + 8 * s, (it >> 1) & 1);
             if (!epi_bar_and(got && ok)) {
-                if (lane == 0) atomicExch(a.err, 1);
+                if (lane == 0) set_err<MULTI>(a0, mu);
                 ok = false;
                 break;
             }
             consumed++;
             tc_fence_after();
+            int tile;
+            const Args &a = file_of<MULTI>(a0, mu, g, tile);
+            const float inv_scale = 1.0f / (MULTI ? operand_scale(a.amax, a.gbound) : scale0);
             const int ci = a.tiles[3 * tile], j0 = a.tiles[3 * tile + 1];
             const int cnt = a.tiles[3 * tile + 2];
             const CsChunk &ch = a.chunks[ci];
@@ -776,6 +830,21 @@ __global__ void __launch_bounds__(nthreads<C>(), 1) search_ws(const __grid_const
         tc_fence_after();
         tmem_dealloc(tmem, TMEM_COLS);
     }
+}
+
+template <class C>
+__global__ void __launch_bounds__(nthreads<C>(), 1) search_ws(const __grid_constant__ Args a)
+{
+    const Multi none = {nullptr, nullptr, 0, 0};
+    ws_body<C, false>(a, none);
+}
+
+/* The same kernel over the tiles of several spectra (search_ws_multi). */
+template <class C>
+__global__ void __launch_bounds__(nthreads<C>(), 1)
+search_ws_multi(const __grid_constant__ Args a0, const __grid_constant__ Multi mu)
+{
+    ws_body<C, true>(a0, mu);
 }
 
 }  // namespace wsk

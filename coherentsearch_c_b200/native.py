@@ -142,6 +142,9 @@ def declare_gpu_api(lib: C.CDLL) -> C.CDLL:
     lib.cs_b200_session_info.restype = C.c_int
     lib.cs_b200_session_device_amps.argtypes = [C.c_void_p]
     lib.cs_b200_session_device_amps.restype = C.c_void_p
+    lib.cs_b200_multi_enqueue.argtypes = [C.POINTER(C.c_void_p), C.c_int,
+                                          C.POINTER(C.c_void_p), C.c_double, C.c_void_p]
+    lib.cs_b200_multi_enqueue.restype = C.c_int
     lib.cs_b200_session_enqueue_device.argtypes = [C.c_void_p, C.c_void_p, C.c_double,
                                                    C.c_void_p]
     lib.cs_b200_session_enqueue_device.restype = C.c_int

@@ -289,3 +289,44 @@ class Session:
             self.close()
         except Exception:
             pass
+
+
+def multi_enqueue(sessions, d_amps=None, threshold: float | None = None, stream=None) -> None:
+    """Queue one persistent launch over the tiles of several spectra
+    (cs_b200_multi_enqueue).  The sessions must share one warp-specialised
+    configuration (nharms, ladder).  d_amps: device spectrum pointers (None:
+    each session's own buffer); stream: a cudaStream_t handle the launch
+    follows (None: the first session's stream)."""
+    gpu = nt.gpu_lib()
+    n = len(sessions)
+    thr = sessions[0].opts.threshold if threshold is None else threshold
+    arr = (C.c_void_p * n)(*[s.sess for s in sessions])
+    amps = None
+    if d_amps is not None:
+        amps = (C.c_void_p * n)(*[int(p) if p else None for p in d_amps])
+    if gpu.cs_b200_multi_enqueue(arr, n, amps, thr, stream) != 0:
+        raise RuntimeError("cs_b200_multi_enqueue failed")
+
+
+def multi_collect(sessions, d_amps=None, threshold: float | None = None):
+    """Each session's raw candidates after multi_enqueue (a session whose
+    record buffer overflowed is searched again on its own)."""
+    thr = sessions[0].opts.threshold if threshold is None else threshold
+    outs, kms = [], 0.0
+    for i, s in enumerate(sessions):
+        out, ms, rc = s.collect(thr)
+        if i == 0:
+            kms = ms
+        if rc == 1:
+            s.enqueue(d_amps[i] if d_amps is not None else None, thr)
+            out, _, rc = s.collect(thr)
+        outs.append(out)
+    return outs, kms
+
+
+def multi_search(sessions, d_amps=None, threshold: float | None = None, stream=None):
+    """multi_enqueue then multi_collect: (list of candidate arrays, kernel ms)."""
+    if not sessions:
+        return [], 0.0
+    multi_enqueue(sessions, d_amps, threshold, stream)
+    return multi_collect(sessions, d_amps, threshold)

@@ -36,6 +36,21 @@ typedef struct {
 
 int cs_b200_session_info(const GpuSession *s, CsB200Info *info);
 
+/* One persistent launch over the tiles of several spectra (no counterpart
+ * in the reference, which searches one file per call): sessions ss[0..n-1],
+ * all FP32 and of one warp-specialised configuration (the same nharms and
+ * decimation ladder at m 16), each with its own geometry, tables and record
+ * buffer.  d_amps[i] is session i's device spectrum (NULL array or entry:
+ * its own buffer).  Each session's spectrum maximum, then one kernel whose
+ * CTAs walk a single list of (spectrum, tile) work items, are queued on
+ * `stream` (NULL: the first session's stream) after the work already queued
+ * on every session's stream; every session's stream then waits for the
+ * launch, so cs_b200_session_collect on each session returns its
+ * candidates, the same as those of its own search.  Calls on one device are
+ * serialised.  Returns 0, or -1 with a message. */
+int cs_b200_multi_enqueue(GpuSession **ss, int n, const float *const *d_amps,
+                          double threshold, void *stream);
+
 /* Device address of the session's spectrum buffer (namps float2). */
 float *cs_b200_session_device_amps(GpuSession *s);
 
