@@ -480,6 +480,13 @@ def run_b200(args):
                                           not args.no_ref_gpu)
         except Exception as exc:   # noqa: BLE001
             line["serve"] = {"unavailable": str(exc)}
+        # the raw-data front end's dedispersion (--workload dedisp has the full
+        # line): 8-bit filterbank, 1024 channels x 2^22 spectra, 500 DMs
+        for name, clipped in (("dedisp", False), ("dedisp_clipped", True)):
+            try:
+                line[name] = dedisp_summary(clipped, local)
+            except Exception as exc:   # noqa: BLE001
+                line[name] = {"unavailable": str(exc)}
     if rank == 0:
         print(json.dumps(line))
     ses.close()
@@ -545,11 +552,40 @@ def dedisp_cpu_rate(raw_host, t, seconds=10.0, clip_sigma=0.0):
 
 
 def run_dedisp(args):
+    world, rank, local, pg = dist_setup(args)
+    line = dedisp_measure(args, world, rank, local, pg)
+    if rank == 0:
+        print(json.dumps(line))
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+def dedisp_summary(clipped, local, steps=5, cpu_seconds=3.0):
+    """The dedispersion workload in short for the search line: DM-samples/s,
+    the two stages' kernel times, and the reference's CPU rate on a sample."""
+    a = argparse.Namespace(clipped=clipped, nspec_log2=0, steps=steps, warmup=3,
+                           no_e2e=True, no_cpu_baseline=False, cpu_seconds=cpu_seconds)
+    line = dedisp_measure(a, 1, 0, local, None)
+    out = {k: line[k] for k in ("value", "unit", "ms_per_step")}
+    out["kernel"] = line["roofline"]["kernel"]
+    out["subband_ms"] = line["roofline"]["subband_ms"]
+    out["dm_ms"] = line["roofline"]["dm_ms"]
+    out["hbm_frac"] = line["roofline"]["frac"]
+    cb = line.get("cpu_baseline", {})
+    out["cpu_baseline"] = cb
+    if cb.get("value"):
+        out["vs_cpu_baseline"] = line["value"] / cb["value"]
+    if clipped:
+        out["spectra_clipped"] = line["spectra_clipped"]
+    return out
+
+
+def dedisp_measure(args, world, rank, local, pg):
     import ctypes as C
     import torch
     from coherentsearch_c_b200 import synth
     from coherentsearch_c_b200.dedisp import Dedisperser, dedisp_tables
-    world, rank, local, pg = dist_setup(args)
     dev = f"cuda:{local}"
     torch.cuda.set_device(local)
     W = dict(DEDISP)
@@ -684,12 +720,9 @@ def run_dedisp(args):
         except Exception as exc:   # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "unit": DEDISP_UNIT, "cores": 0,
                                     "kind": "reference", "sample": f"unavailable: {exc}"}
-    if rank == 0:
-        print(json.dumps(line))
     dd.close()
-    if pg is not None:
-        pg.destroy_process_group()
-    return 0
+    torch.cuda.set_stream(torch.cuda.default_stream(dev))
+    return line
 
 
 def prep_cpu_rate(series_host, dd_rate, N, dt, opts, seconds=10.0):
