@@ -966,7 +966,8 @@ def sweep_lines(files, slots, nh_list, steps, warmup, ref_gpu, device=0):
     import torch
     from coherentsearch_c_b200 import synth
     from coherentsearch_c_b200.batch import Batch
-    from coherentsearch_c_b200.search import Options, Session
+    from coherentsearch_c_b200 import native as nt
+    from coherentsearch_c_b200.search import Options, Session, multi_search
     from coherentsearch_c_b200.sweep import autotune, search_list, warm
     specs = synth.config_dm_sweep(n_files=files)
     dt = specs[0].dt
@@ -1028,6 +1029,29 @@ def sweep_lines(files, slots, nh_list, steps, warmup, ref_gpu, device=0):
                 e1.synchronize()
                 ts.append(e0.elapsed_time(e1))
             res[name] = (statistics.mean(ts), out)
+        # every spectrum resident on the device, searched by ONE persistent
+        # launch over all their tiles (the kernel-side bound of the grouped form)
+        for i in range(len(specs)):
+            upload(i)
+        resident = [Session(sp.N, dt, opts, device=device) for sp in specs]
+        ptrs = [b.data_ptr() for b in dev_bufs]
+        try:
+            multi_search(resident, ptrs, stream=st)                # warm
+            rts, rks = [], []
+            for _ in range(max(1, min(steps, 2))):
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                rout, kms = multi_search(resident, ptrs, stream=st)
+                e1.record(stream)
+                e1.synchronize()
+                rts.append(e0.elapsed_time(e1))
+                rks.append(kms)
+        finally:
+            for ses in resident:
+                ses.close()
+            nt.gpu_lib().cs_b200_session_park_drain()
         diff = [i for i, (x, y) in enumerate(zip(res["plain"][1], res["batched"][1]))
                 if not _same_cands(x, y)]
         equal = not diff
@@ -1042,6 +1066,11 @@ def sweep_lines(files, slots, nh_list, steps, warmup, ref_gpu, device=0):
                      "autotune_seconds_by_group": {str(k): v for k, v in tune.items()},
                      "grouped_equal_candidates": bool(all(
                          _same_cands(x, y) for x, y in zip(res["grouped"][1], res["plain"][1]))),
+                     "resident_one_launch_ms": statistics.mean(rts),
+                     "resident_one_launch_trials_per_s": trials / (statistics.mean(rts) * 1e-3),
+                     "resident_one_launch_kernel_ms": statistics.mean(rks),
+                     "resident_equal_candidates": bool(all(
+                         _same_cands(x, y) for x, y in zip(rout, res["plain"][1]))),
                      "equal_candidates": bool(equal), "differing_files": diff,
                      "candidates": int(sum(o.size for o in res["batched"][1])),
                      "plain_candidates": int(sum(o.size for o in res["plain"][1]))}

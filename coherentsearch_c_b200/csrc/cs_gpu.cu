@@ -1045,12 +1045,20 @@ static int ws_smem(int nh)
                     : wsk::smem_bytes<wsk::Cfg16>();
 }
 
+static int ws_smem_multi(int nh)
+{
+    return nh == 60 ? wsk::smem_bytes_multi<wsk::Cfg60>()
+         : nh == 32 ? wsk::smem_bytes_multi<wsk::Cfg32>()
+                    : wsk::smem_bytes_multi<wsk::Cfg16>();
+}
+
 static cudaError_t ws_prepare_multi(int nh)
 {
     const void *fn = nh == 60 ? (const void *)wsk::search_ws_multi<wsk::Cfg60>
                    : nh == 32 ? (const void *)wsk::search_ws_multi<wsk::Cfg32>
                               : (const void *)wsk::search_ws_multi<wsk::Cfg16>;
-    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, ws_smem(nh));
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                ws_smem_multi(nh));
 }
 
 static cudaError_t ws_prepare(int nh)
@@ -1798,12 +1806,9 @@ CS_EXPORT int cs_b200_session_sync(GpuSession *S)
 /* ------------------------------------------------------------------ */
 /* Several spectra in one launch (cs_b200_multi_enqueue)               */
 /* ------------------------------------------------------------------ */
-/* Per device: the launch's argument table and tile offsets (grow-only), and
- * an event marking the last launch that read them. */
+/* Per device: an event marking the last launch that read the kernel's
+ * constant-memory tables (arguments and tile offsets). */
 struct MultiTables {
-    wsk::Args *d_files;
-    int *d_off;
-    size_t cap;
     cudaEvent_t done;
 };
 static std::mutex g_multi_mu;
@@ -1820,7 +1825,7 @@ static cudaError_t multi_launch(int nh, int grid, cudaStream_t st, const wsk::Ar
     wsk::Args a = a0;
     wsk::Multi m = mu;
     void *args[2] = {&a, &m};
-    return cudaLaunchKernel(fn, dim3(grid), dim3(nthr), args, (size_t)ws_smem(nh), st);
+    return cudaLaunchKernel(fn, dim3(grid), dim3(nthr), args, (size_t)ws_smem_multi(nh), st);
 }
 
 CS_EXPORT int cs_b200_multi_enqueue(GpuSession **ss, int n, const float *const *d_amps,
@@ -1836,6 +1841,11 @@ CS_EXPORT int cs_b200_multi_enqueue(GpuSession **ss, int n, const float *const *
         }                                                                         \
     } while (0)
     if (!ss || n < 1) return -1;
+    if (n > wsk::MULTI_MAX) {
+        fprintf(stderr, "Error: a multi-spectrum launch takes at most %d spectra (got %d)\n",
+                wsk::MULTI_MAX, n);
+        return -1;
+    }
     GpuSession *S0 = ss[0];
     for (int i = 0; i < n; i++) {
         const GpuSession *S = ss[i];
@@ -1880,25 +1890,12 @@ CS_EXPORT int cs_b200_multi_enqueue(GpuSession **ss, int n, const float *const *
     if (ntiles <= 0) return 0;
     /* the previous launch on this device may still read the tables */
     MCK(cudaStreamWaitEvent(st, M.done, 0));
-    if ((size_t)n > M.cap) {
-        MCK(cudaStreamSynchronize(st));
-        cudaFree(M.d_files);
-        cudaFree(M.d_off);
-        M.d_files = NULL;
-        M.d_off = NULL;
-        M.cap = 0;
-        const size_t cap = (size_t)n + 16;
-        MCK(cudaMalloc((void **)&M.d_files, cap * sizeof(wsk::Args)));
-        MCK(cudaMalloc((void **)&M.d_off, (cap + 1) * sizeof(int)));
-        M.cap = cap;
-    }
     /* pageable sources: each copy returns once its data is staged */
-    MCK(cudaMemcpyAsync(M.d_files, files.data(), files.size() * sizeof(wsk::Args),
-                        cudaMemcpyHostToDevice, st));
-    MCK(cudaMemcpyAsync(M.d_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    MCK(cudaMemcpyToSymbolAsync(wsk::c_multi_files, files.data(),
+                                files.size() * sizeof(wsk::Args), 0, cudaMemcpyHostToDevice, st));
+    MCK(cudaMemcpyToSymbolAsync(wsk::c_multi_off, off.data(), off.size() * sizeof(int), 0,
+                                cudaMemcpyHostToDevice, st));
     wsk::Multi mu;
-    mu.files = M.d_files;
-    mu.tile_off = M.d_off;
     mu.nfiles = n;
     mu.ntiles = ntiles;
     const int grid = std::min(ntiles, S0->nsm);

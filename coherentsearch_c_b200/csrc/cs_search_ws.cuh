@@ -582,45 +582,75 @@ __host__ __device__ constexpr int smem_bytes()
     return 2 * C::NPAD * C::KPAD * 2 + 64 + 16 + C::NH * (int)sizeof(Harm);
 }
 
+/* harmonic headers of the first MULTI_HCACHE spectra of a CTA's tile run,
+ * copied to shared memory; later ones are read from global memory */
+constexpr int MULTI_HCACHE = 8;
+
+/* the multi-spectrum kernel adds the header cache */
+template <class C>
+__host__ __device__ constexpr int smem_bytes_multi()
+{
+    return smem_bytes<C>() + MULTI_HCACHE * C::NH * (int)sizeof(Harm);
+}
+
 /* Several spectra of the same configuration in one persistent launch: a
- * device table of per-spectrum arguments and the prefix sums of their tile
- * counts.  Each tile finds its spectrum (binary search) and takes that
- * spectrum's tables, operand scale and record buffer. */
+ * table of per-spectrum arguments (c_multi_files) and the prefix sums of
+ * their tile counts (c_multi_off).  Each tile takes its spectrum's tables,
+ * operand scale and record buffer. */
 struct Multi {
-    const Args *files;
-    const int *tile_off;        /* nfiles + 1 */
     int nfiles;
     int ntiles;
 };
 
-/* The arguments and local tile index of global tile g. */
-template <bool MULTI>
-static __device__ __forceinline__ const Args &file_of(const Args &a0, const Multi &mu, int g,
-                                                      int &tile)
+/* Both tables live in constant memory.  Every index into them is uniform
+ * over the CTA (derived from the tile loop and the tables alone), so the
+ * per-spectrum fields are broadcast reads held in uniform registers, as
+ * cheap as kernel parameters, and stay off the L1 load path the
+ * interpolation is bound on.  Launches on one device are serialised by the
+ * host. */
+constexpr int MULTI_MAX = 400;
+__constant__ Args c_multi_files[MULTI_MAX];
+__constant__ int c_multi_off[MULTI_MAX + 1];
+
+/* The spectrum of global tile g (binary search over the tile offsets). */
+static __device__ __forceinline__ int file_search(const Multi &mu, int g)
 {
-    if (!MULTI) {
-        tile = g;
-        return a0;
-    }
     int lo = 0, hi = mu.nfiles - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(mu.tile_off + mid) <= g) lo = mid;
+        if (c_multi_off[mid] <= g) lo = mid;
         else hi = mid - 1;
     }
-    tile = g - __ldg(mu.tile_off + lo);
-    return mu.files[lo];
+    return lo;
+}
+
+/* A role's cursor over its CTA's tile run: tiles come in increasing order,
+ * so the spectrum index only moves forward.  Returns the local tile index
+ * of global tile g and leaves f at its spectrum. */
+template <bool MULTI>
+static __device__ __forceinline__ int file_step(int &f, int g)
+{
+    if (!MULTI) return g;
+    while (g >= c_multi_off[f + 1]) f++;
+    return g - c_multi_off[f];
+}
+
+template <bool MULTI>
+static __device__ __forceinline__ const Args &file_args(const Args &a0, int f)
+{
+    if (!MULTI) return a0;
+    return c_multi_files[f];
 }
 
 /* A failed wait: every spectrum of the launch reports the error. */
 template <bool MULTI>
 static __device__ __forceinline__ void set_err(const Args &a0, const Multi &mu)
 {
-    if (!MULTI) {
+    if constexpr (!MULTI) {
         atomicExch(a0.err, 1);
-        return;
+    } else {
+        for (int f = 0; f < mu.nfiles; f++) atomicExch(c_multi_files[f].err, 1);
     }
-    for (int f = 0; f < mu.nfiles; f++) atomicExch(mu.files[f].err, 1);
 }
 
 template <class C, bool MULTI>
@@ -644,10 +674,27 @@ static __device__ __forceinline__ void ws_body(const Args &a0, const Multi &mu)
     const uint32_t bar_dfull = bar_afull + 32;
     uint32_t *tm_slot = reinterpret_cast<uint32_t *>(smem + SM_TM);
     Harm *hs = reinterpret_cast<Harm *>(smem + SM_HARM);
+    Harm *hcache = hs + NH;                          /* MULTI: [MULTI_HCACHE][NH] */
+    /* each CTA owns a contiguous run of tiles: neighbouring tiles read the
+     * same spectral windows and weight rows, which then stay in L1 */
+    const int ntiles = MULTI ? mu.ntiles : a0.ntiles;
+    const int per_cta = (ntiles + gridDim.x - 1) / gridDim.x;
+    const int tile_begin = min(ntiles, (int)blockIdx.x * per_cta);
+    const int tile_end = min(ntiles, tile_begin + per_cta);
+    int f_first = 0;
+    if (MULTI && tile_begin < tile_end) {
+        f_first = file_search(mu, tile_begin);
+    }
 
     if (warp == 0) tmem_alloc(smem_u32(tm_slot), TMEM_COLS);
-    if (!MULTI)
+    if (!MULTI) {
         for (int h = tid; h < NH; h += NTHREADS) hs[h] = a0.harm[h];
+    } else {
+        for (int i = tid; i < MULTI_HCACHE * NH; i += NTHREADS) {
+            const int f = f_first + i / NH;
+            if (f < mu.nfiles) hcache[i] = c_multi_files[f].harm[i % NH];
+        }
+    }
     if (tid == 0) {
         mbar_init(bar_afull, NIW + 8);      /* every interpolation and epilogue warp */
         mbar_init(bar_afull + 8, NIW + 8);
@@ -667,13 +714,6 @@ static __device__ __forceinline__ void ws_body(const Args &a0, const Multi &mu)
     const uint32_t tmem = *tm_slot;
     /* the fp16 operand scale of a spectrum (one per launch unless MULTI) */
     const float scale0 = MULTI ? 1.0f : operand_scale(a0.amax, a0.gbound);
-    /* each CTA owns a contiguous run of tiles: neighbouring tiles read the
-     * same spectral windows and weight rows, which then stay in L1 */
-    const int ntiles = MULTI ? mu.ntiles : a0.ntiles;
-    const int per_cta = (ntiles + gridDim.x - 1) / gridDim.x;
-    const int tile_begin = min(ntiles, (int)blockIdx.x * per_cta);
-    const int tile_end = min(ntiles, tile_begin + per_cta);
-
     if (warp < NIW) {
         /* --------------- interpolation of blocks 0..HEAD-1 --------------- */
         const int r = tid & (CS_TILE_M - 1);
@@ -691,7 +731,7 @@ static __device__ __forceinline__ void ws_body(const Args &a0, const Multi &mu)
                 }
             }
         }
-        int it = 0;
+        int it = 0, f = f_first;
         for (int g = tile_begin; g < tile_end; g++, it++) {
             const int s = it & 1;
             if (it >= 2 && !mbar_wait(bar_aempty + 8 * s, ((it - 2) >> 1) & 1)) {
@@ -699,9 +739,10 @@ static __device__ __forceinline__ void ws_body(const Args &a0, const Multi &mu)
                 break;
             }
             tc_fence_after();
-            int tile;
-            const Args &a = file_of<MULTI>(a0, mu, g, tile);
-            const Harm *hsp = MULTI ? a.harm : hs;
+            const int tile = file_step<MULTI>(f, g);
+            const Args &a = file_args<MULTI>(a0, f);
+            const Harm *hsp = !MULTI ? hs
+                            : (f - f_first < MULTI_HCACHE ? hcache + (f - f_first) * NH : a.harm);
             const float scale = MULTI ? operand_scale(a.amax, a.gbound) : scale0;
             const TrialState ts = trial_state(a, tile, r);
             const uint32_t abuf = tmem + tlane + (uint32_t)(TM_A + KPAD * s);
@@ -735,10 +776,13 @@ static __device__ __forceinline__ void ws_body(const Args &a0, const Multi &mu)
         int issued = 0, consumed = 0;
         bool ok = true;
 
+        int ft = f_first, fe = f_first;      /* cursors of the tail and the epilogue */
         auto tail = [&](int it, int g) {
-            int tile;
-            const Args &a = file_of<MULTI>(a0, mu, g, tile);
-            const Harm *hsp = MULTI ? a.harm : hs;
+            const int tile = file_step<MULTI>(ft, g);
+            const int f = ft;
+            const Args &a = file_args<MULTI>(a0, f);
+            const Harm *hsp = !MULTI ? hs
+                            : (f - f_first < MULTI_HCACHE ? hcache + (f - f_first) * NH : a.harm);
             const float scale = MULTI ? operand_scale(a.amax, a.gbound) : scale0;
             const TrialState ts = trial_state(a, tile, r);
             const uint32_t abuf = tmem + tlane + (uint32_t)(TM_A + KPAD * (it & 1));
@@ -806,8 +850,8 @@ static __device__ __forceinline__ void ws_body(const Args &a0, const Multi &mu)
             }
             consumed++;
             tc_fence_after();
-            int tile;
-            const Args &a = file_of<MULTI>(a0, mu, g, tile);
+            const int tile = file_step<MULTI>(fe, g);
+            const Args &a = file_args<MULTI>(a0, fe);
             const float inv_scale = 1.0f / (MULTI ? operand_scale(a.amax, a.gbound) : scale0);
             const int ci = a.tiles[3 * tile], j0 = a.tiles[3 * tile + 1];
             const int cnt = a.tiles[3 * tile + 2];
@@ -835,7 +879,7 @@ static __device__ __forceinline__ void ws_body(const Args &a0, const Multi &mu)
 template <class C>
 __global__ void __launch_bounds__(nthreads<C>(), 1) search_ws(const __grid_constant__ Args a)
 {
-    const Multi none = {nullptr, nullptr, 0, 0};
+    const Multi none = {0, 0};
     ws_body<C, false>(a, none);
 }
 

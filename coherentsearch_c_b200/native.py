@@ -13,7 +13,8 @@ import os
 import numpy as np
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIBDIR = os.path.join(PKG, "lib")
+# the built libraries; CS_B200_LIBDIR points at another build of them
+LIBDIR = os.environ.get("CS_B200_LIBDIR") or os.path.join(PKG, "lib")
 
 
 class SimpleInf(C.Structure):
