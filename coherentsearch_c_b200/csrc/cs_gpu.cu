@@ -1898,6 +1898,9 @@ CS_EXPORT int cs_b200_multi_enqueue(GpuSession **ss, int n, const float *const *
     wsk::Multi mu;
     mu.nfiles = n;
     mu.ntiles = ntiles;
+    /* tiles per CTA block (the kernel's schedule); CS_B200_MULTI_BLOCK tunes it */
+    mu.block = 64;
+    if (const char *e = getenv("CS_B200_MULTI_BLOCK")) mu.block = std::max(1, atoi(e));
     const int grid = std::min(ntiles, S0->nsm);
     MCK(cudaEventRecord(S0->ev0, st));
     MCK(multi_launch(S0->use_ws, grid, st, files[0], mu));

@@ -582,24 +582,29 @@ __host__ __device__ constexpr int smem_bytes()
     return 2 * C::NPAD * C::KPAD * 2 + 64 + 16 + C::NH * (int)sizeof(Harm);
 }
 
-/* harmonic headers of the first MULTI_HCACHE spectra of a CTA's tile run,
- * copied to shared memory; later ones are read from global memory */
-constexpr int MULTI_HCACHE = 8;
-
-/* the multi-spectrum kernel adds the header cache */
+/* the multi-spectrum kernel adds one header slot per warp */
 template <class C>
 __host__ __device__ constexpr int smem_bytes_multi()
 {
-    return smem_bytes<C>() + MULTI_HCACHE * C::NH * (int)sizeof(Harm);
+    return smem_bytes<C>() + (C::NIW + 8) * C::NH * (int)sizeof(Harm);
 }
 
 /* Several spectra of the same configuration in one persistent launch: a
  * table of per-spectrum arguments (c_multi_files) and the prefix sums of
  * their tile counts (c_multi_off).  Each tile takes its spectrum's tables,
- * operand scale and record buffer. */
+ * operand scale and record buffer.
+ *
+ * Schedule: rounds of grid x `block` consecutive tiles of the concatenated
+ * list; in each round CTA b takes the b-th block of `block` tiles, and the
+ * last, partial round is split evenly (to one tile) over the CTAs.  At any
+ * time every CTA works inside the same few spectra, so the L2 holds their
+ * windows and weight rows as it does for one spectrum (CTA-contiguous runs
+ * over a long list put every CTA in a different spectrum, a working set of
+ * many spectra); within a block neighbouring tiles still share L1 lines. */
 struct Multi {
     int nfiles;
     int ntiles;
+    int block;
 };
 
 /* Both tables live in constant memory.  Every index into them is uniform
@@ -612,35 +617,91 @@ constexpr int MULTI_MAX = 400;
 __constant__ Args c_multi_files[MULTI_MAX];
 __constant__ int c_multi_off[MULTI_MAX + 1];
 
-/* The spectrum of global tile g (binary search over the tile offsets). */
-static __device__ __forceinline__ int file_search(const Multi &mu, int g)
+/* A role's walk over its CTA's tiles: g the global tile, end the end of the
+ * current run (single spectrum: the CTA's contiguous run; several: the
+ * current block), f the spectrum of g.  Tiles come in increasing order, so
+ * f only moves forward. */
+struct Walk {
+    int g, end, f, base;
+};
+
+/* The CTA's block of the round starting at tile w.base (false: none). */
+static __device__ __forceinline__ bool walk_block(Walk &w, const Multi &mu)
 {
-    int lo = 0, hi = mu.nfiles - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (c_multi_off[mid] <= g) lo = mid;
-        else hi = mid - 1;
+    const int G = (int)gridDim.x, b = (int)blockIdx.x;
+    if (w.base >= mu.ntiles) return false;
+    const int rem = mu.ntiles - w.base;
+    if (rem >= G * mu.block) {
+        w.g = w.base + b * mu.block;
+        w.end = w.g + mu.block;
+    } else {
+        w.g = w.base + (int)(((long long)b * rem) / G);
+        w.end = w.base + (int)(((long long)(b + 1) * rem) / G);
     }
-    return lo;
-}
-
-/* A role's cursor over its CTA's tile run: tiles come in increasing order,
- * so the spectrum index only moves forward.  Returns the local tile index
- * of global tile g and leaves f at its spectrum. */
-template <bool MULTI>
-static __device__ __forceinline__ int file_step(int &f, int g)
-{
-    if (!MULTI) return g;
-    while (g >= c_multi_off[f + 1]) f++;
-    return g - c_multi_off[f];
+    return w.g < w.end;
 }
 
 template <bool MULTI>
-static __device__ __forceinline__ const Args &file_args(const Args &a0, int f)
+static __device__ __forceinline__ bool walk_begin(Walk &w, const Multi &mu, int tile_begin,
+                                                  int tile_end)
 {
-    if (!MULTI) return a0;
-    return c_multi_files[f];
+    w.f = 0;
+    if (!MULTI) {
+        w.g = tile_begin;
+        w.end = tile_end;
+        return w.g < w.end;
+    }
+    w.base = 0;
+    return walk_block(w, mu);
 }
+
+template <bool MULTI>
+static __device__ __forceinline__ bool walk_next(Walk &w, const Multi &mu)
+{
+    if (++w.g < w.end) return true;
+    if (!MULTI) return false;
+    w.base += (int)gridDim.x * mu.block;
+    return walk_block(w, mu);
+}
+
+/* The local tile index of the walk's tile; moves w.f to its spectrum. */
+template <bool MULTI>
+static __device__ __forceinline__ int walk_tile(Walk &w)
+{
+    if (!MULTI) return w.g;
+    while (w.g >= c_multi_off[w.f + 1]) w.f++;
+    return w.g - c_multi_off[w.f];
+}
+
+/* A warp's private copy of spectrum f's harmonic headers (shared memory,
+ * refreshed when the warp's walk enters another spectrum; no other warp
+ * reads it, so a __syncwarp on both sides orders it). */
+template <int NH>
+static __device__ __forceinline__ void load_headers(Harm *slot, int f, int lane)
+{
+    __syncwarp();
+    const int *src = reinterpret_cast<const int *>(c_multi_files[f].harm);
+    int *dst = reinterpret_cast<int *>(slot);
+    constexpr int NW = NH * (int)sizeof(Harm) / 4;
+    for (int i = lane; i < NW; i += 32) dst[i] = __ldg(src + i);
+    __syncwarp();
+}
+
+/* The arguments of a tile: the launch's own, or (MULTI) its spectrum's entry
+ * of the constant table.  For nharms 60 the entry is copied out once per
+ * tile, so that the fields the harmonic loop reads sit in registers instead
+ * of being re-read from the table inside it (measured: 1.63 -> 1.68 G
+ * trials/s); the smaller configurations run faster reading the table
+ * (their extra registers cost more than the reads).  Bit k of
+ * WSK_MULTI_COPY selects the copy for configuration k (16, 32, 60). */
+#ifndef WSK_MULTI_COPY
+#define WSK_MULTI_COPY 4
+#endif
+#define WS_TILE_ARGS(a, f)                                                       \
+    constexpr bool a##_cp = MULTI && ((WSK_MULTI_COPY >> (NH == 16 ? 0 : NH == 32 ? 1 : 2)) & 1); \
+    Args a##_copy;                                                               \
+    if constexpr (a##_cp) a##_copy = c_multi_files[(f)];                         \
+    const Args &a = a##_cp ? a##_copy : MULTI ? c_multi_files[(f)] : a0
 
 /* A failed wait: every spectrum of the launch reports the error. */
 template <bool MULTI>
@@ -674,27 +735,17 @@ static __device__ __forceinline__ void ws_body(const Args &a0, const Multi &mu)
     const uint32_t bar_dfull = bar_afull + 32;
     uint32_t *tm_slot = reinterpret_cast<uint32_t *>(smem + SM_TM);
     Harm *hs = reinterpret_cast<Harm *>(smem + SM_HARM);
-    Harm *hcache = hs + NH;                          /* MULTI: [MULTI_HCACHE][NH] */
-    /* each CTA owns a contiguous run of tiles: neighbouring tiles read the
-     * same spectral windows and weight rows, which then stay in L1 */
-    const int ntiles = MULTI ? mu.ntiles : a0.ntiles;
-    const int per_cta = (ntiles + gridDim.x - 1) / gridDim.x;
-    const int tile_begin = min(ntiles, (int)blockIdx.x * per_cta);
-    const int tile_end = min(ntiles, tile_begin + per_cta);
-    int f_first = 0;
-    if (MULTI && tile_begin < tile_end) {
-        f_first = file_search(mu, tile_begin);
-    }
+    Harm *hslot = hs + NH * (1 + warp);              /* MULTI: this warp's headers */
+    /* one spectrum: each CTA owns a contiguous run of tiles (neighbouring
+     * tiles read the same spectral windows and weight rows, which then stay
+     * in L1); several: the block-cyclic walk of struct Multi */
+    const int per_cta = (a0.ntiles + gridDim.x - 1) / gridDim.x;
+    const int tile_begin = MULTI ? 0 : min(a0.ntiles, (int)blockIdx.x * per_cta);
+    const int tile_end = MULTI ? 0 : min(a0.ntiles, tile_begin + per_cta);
 
     if (warp == 0) tmem_alloc(smem_u32(tm_slot), TMEM_COLS);
-    if (!MULTI) {
+    if (!MULTI)
         for (int h = tid; h < NH; h += NTHREADS) hs[h] = a0.harm[h];
-    } else {
-        for (int i = tid; i < MULTI_HCACHE * NH; i += NTHREADS) {
-            const int f = f_first + i / NH;
-            if (f < mu.nfiles) hcache[i] = c_multi_files[f].harm[i % NH];
-        }
-    }
     if (tid == 0) {
         mbar_init(bar_afull, NIW + 8);      /* every interpolation and epilogue warp */
         mbar_init(bar_afull + 8, NIW + 8);
@@ -731,19 +782,25 @@ static __device__ __forceinline__ void ws_body(const Args &a0, const Multi &mu)
                 }
             }
         }
-        int it = 0, f = f_first;
-        for (int g = tile_begin; g < tile_end; g++, it++) {
+        Walk w;
+        int fcur = -1;
+        float scale = scale0;
+        bool more = walk_begin<MULTI>(w, mu, tile_begin, tile_end);
+        for (int it = 0; more; it++, more = walk_next<MULTI>(w, mu)) {
             const int s = it & 1;
             if (it >= 2 && !mbar_wait(bar_aempty + 8 * s, ((it - 2) >> 1) & 1)) {
                 if (lane == 0) set_err<MULTI>(a0, mu);
                 break;
             }
             tc_fence_after();
-            const int tile = file_step<MULTI>(f, g);
-            const Args &a = file_args<MULTI>(a0, f);
-            const Harm *hsp = !MULTI ? hs
-                            : (f - f_first < MULTI_HCACHE ? hcache + (f - f_first) * NH : a.harm);
-            const float scale = MULTI ? operand_scale(a.amax, a.gbound) : scale0;
+            const int tile = walk_tile<MULTI>(w);
+            WS_TILE_ARGS(a, w.f);
+            if (MULTI && w.f != fcur) {
+                fcur = w.f;
+                load_headers<NH>(hslot, fcur, lane);
+                scale = operand_scale(a.amax, a.gbound);
+            }
+            const Harm *hsp = MULTI ? hslot : hs;
             const TrialState ts = trial_state(a, tile, r);
             const uint32_t abuf = tmem + tlane + (uint32_t)(TM_A + KPAD * s);
             uint32_t res, qint, r4, q4;
@@ -776,14 +833,21 @@ static __device__ __forceinline__ void ws_body(const Args &a0, const Multi &mu)
         int issued = 0, consumed = 0;
         bool ok = true;
 
-        int ft = f_first, fe = f_first;      /* cursors of the tail and the epilogue */
-        auto tail = [&](int it, int g) {
-            const int tile = file_step<MULTI>(ft, g);
-            const int f = ft;
-            const Args &a = file_args<MULTI>(a0, f);
-            const Harm *hsp = !MULTI ? hs
-                            : (f - f_first < MULTI_HCACHE ? hcache + (f - f_first) * NH : a.harm);
-            const float scale = MULTI ? operand_scale(a.amax, a.gbound) : scale0;
+        /* walks of the tail blocks (one tile ahead) and of the epilogue, with
+         * the spectrum and operand scale each last saw */
+        Walk wt, we;
+        int ft_cur = -1, fe_cur = -1;
+        float scale_t = scale0, inv_scale = 1.0f / scale0;
+        auto tail = [&](int it) {
+            const int tile = walk_tile<MULTI>(wt);
+            WS_TILE_ARGS(a, wt.f);
+            if (MULTI && wt.f != ft_cur) {
+                ft_cur = wt.f;
+                load_headers<NH>(hslot, ft_cur, lane);
+                scale_t = operand_scale(a.amax, a.gbound);
+            }
+            const Harm *hsp = MULTI ? hslot : hs;
+            const float scale = scale_t;
             const TrialState ts = trial_state(a, tile, r);
             const uint32_t abuf = tmem + tlane + (uint32_t)(TM_A + KPAD * (it & 1));
             uint32_t res, qint;
@@ -819,8 +883,10 @@ static __device__ __forceinline__ void ws_body(const Args &a0, const Multi &mu)
         };
 
         /* tile 0: its tail blocks, then its MMAs */
-        if (tile_begin < tile_end) {
-            tail(0, tile_begin);
+        bool tmore = walk_begin<MULTI>(wt, mu, tile_begin, tile_end);
+        bool emore = walk_begin<MULTI>(we, mu, tile_begin, tile_end);
+        if (tmore) {
+            tail(0);
             if (leader) {
                 ok = issue(0);
                 if (ok) issued = 1;
@@ -828,13 +894,13 @@ static __device__ __forceinline__ void ws_body(const Args &a0, const Multi &mu)
             }
             __syncwarp();
         }
-        int it = 0;
-        for (int g = tile_begin; g < tile_end; g++, it++) {
+        for (int it = 0; emore; it++, emore = walk_next<MULTI>(we, mu)) {
             const int s = it & 1;
-            if (g + 1 < tile_end) {
+            tmore = tmore && walk_next<MULTI>(wt, mu);
+            if (tmore) {
                 /* A buffer (it+1)&1 was last read by the MMA of tile it-1, whose
                  * accumulator this group already consumed: it is free */
-                tail(it + 1, g + 1);
+                tail(it + 1);
                 if (leader && ok) {
                     ok = issue(it + 1);
                     if (ok) issued++;
@@ -850,9 +916,13 @@ static __device__ __forceinline__ void ws_body(const Args &a0, const Multi &mu)
             }
             consumed++;
             tc_fence_after();
-            const int tile = file_step<MULTI>(fe, g);
-            const Args &a = file_args<MULTI>(a0, fe);
-            const float inv_scale = 1.0f / (MULTI ? operand_scale(a.amax, a.gbound) : scale0);
+            const int tile = walk_tile<MULTI>(we);
+            /* the epilogue reads few fields: a reference into the table */
+            const Args &a = MULTI ? c_multi_files[we.f] : a0;
+            if (MULTI && we.f != fe_cur) {
+                fe_cur = we.f;
+                inv_scale = 1.0f / operand_scale(a.amax, a.gbound);
+            }
             const int ci = a.tiles[3 * tile], j0 = a.tiles[3 * tile + 1];
             const int cnt = a.tiles[3 * tile + 2];
             const CsChunk &ch = a.chunks[ci];
@@ -879,7 +949,7 @@ static __device__ __forceinline__ void ws_body(const Args &a0, const Multi &mu)
 template <class C>
 __global__ void __launch_bounds__(nthreads<C>(), 1) search_ws(const __grid_constant__ Args a)
 {
-    const Multi none = {0, 0};
+    const Multi none = {0, 0, 1};
     ws_body<C, false>(a, none);
 }
 
