@@ -63,6 +63,11 @@ class Options:
         return r_lo, lodr, max(total, 0)
 
 
+_libc_free = C.CDLL(None).free
+_libc_free.argtypes = [C.c_void_p]
+_libc_free.restype = None
+
+
 def _as_amps(amps) -> np.ndarray:
     a = np.ascontiguousarray(amps)
     if a.dtype == np.complex64:
@@ -127,8 +132,10 @@ class Session:
         if self.total <= 0:
             raise ValueError("empty trial range")
         self.namps = N // 2
-        self._dummy = np.zeros(2 * self.namps, dtype=np.float32)
+        # planning reads the geometry only (N, namps, T), never the amplitudes
+        self._dummy = np.zeros(2, dtype=np.float32)
         self.ft = _file(self._dummy, N, dt)
+        self.ft.namps = self.namps
         self.plans = nt.DirectPlanSet()
         if self.host.direct_plans_build(C.byref(self.plans), C.byref(self.params), self.r_lo):
             raise RuntimeError("direct_plans_build failed")
@@ -139,7 +146,7 @@ class Session:
             raise RuntimeError("chunk_starts failed")
         self.nchunks = nch.value
         self.cstarts = np.ctypeslib.as_array(cs, shape=(self.nchunks,)).copy()
-        C.CDLL(None).free(cs)
+        _libc_free(cs)
         self._cs = self.cstarts.ctypes.data_as(C.POINTER(C.c_longlong))
         self.sess = self.gpu.cs_gpu_session_create(
             C.byref(self.ft), C.byref(self.params), C.byref(self.plans), self._cs, self.total,
