@@ -73,23 +73,27 @@
 namespace dd {
 
 /* tile shapes (compile-time; DD_* override them for tuning builds) */
-#ifndef DD_DM_TT
-#define DD_DM_TT 256
-#endif
-#ifndef DD_DM_GD
-#define DD_DM_GD 4
-#endif
 #ifndef DD_SB_TT
 #define DD_SB_TT 256
 #endif
+#ifndef DD_DM_NCW
+#define DD_DM_NCW 16
+#endif
 constexpr int SB_TT = DD_SB_TT;   /* samples per subband tile */
 constexpr int SB_THREADS = 512;
-constexpr int DM_TT = DD_DM_TT;   /* samples per DM tile */
-constexpr int DM_G = 32;          /* most DMs per group (one CTA) */
-constexpr int DM_R = 8;           /* samples (4 pairs) per thread */
-constexpr int DM_GD = DD_DM_GD;   /* DMs per thread */
-constexpr int DM_THREADS = (DM_TT / DM_R) * (DM_G / DM_GD);
-static_assert(DM_THREADS <= 1024 && DM_G % DM_GD == 0, "DM tile shape");
+/* S word w of a subband holds samples w and w + DM_P (low, high half), so a
+ * DM tile of 2 DM_P samples reads one aligned word per (DM, subband, column)
+ * whatever the parity of the DM's offset */
+constexpr int DM_P = 128;
+constexpr int DM_TILE = 2 * DM_P; /* samples per DM tile */
+constexpr int DM_G = 32;          /* most DMs per group (one work item) */
+constexpr int DM_NCW = DD_DM_NCW; /* summing warps of the DM stage */
+constexpr int DM_DPT = DM_G / DM_NCW;   /* most DMs a summing thread */
+constexpr int DM_CPT = DM_P / 32;       /* columns a summing thread */
+constexpr int DM_THREADS = (DM_NCW + 1) * 32;   /* + one copy warp */
+constexpr int DM_MAXST = 4;       /* most pipeline stages */
+static_assert(DM_G % DM_NCW == 0 && DM_P % 32 == 0, "DM tile shape");
+constexpr unsigned long long DD_WAIT_NS = 2000000000ull;   /* bound on any in-kernel wait */
 
 static __device__ __forceinline__ uint32_t smem_addr(const void *p)
 {
@@ -116,6 +120,64 @@ static __device__ __forceinline__ void cp_async_wait_all()
     asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+/* mbarriers and bulk copies (one elected thread arms a barrier with the
+ * bytes it expects; the copy engine completes them) */
+static __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+static __device__ __forceinline__ void mbar_fence_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+static __device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+static __device__ __forceinline__ void mbar_arrive_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+
+static __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+    return ok != 0;
+}
+
+/* Bounded wait for the phase of the given parity (false after DD_WAIT_NS). */
+static __device__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    if (mbar_try(bar, parity)) return true;
+    unsigned long long t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    while (!mbar_try(bar, parity)) {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 > DD_WAIT_NS) return false;
+        __nanosleep(32);
+    }
+    return true;
+}
+
+/* Global -> shared bulk copy (16-byte aligned ends, a multiple of 16 bytes)
+ * completing `bytes` on barrier bar. */
+static __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                                uint32_t bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+                 "[%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
 /* ---------------------------------------------------------------- */
 /* Subband stage                                                     */
 /* ---------------------------------------------------------------- */
@@ -130,7 +192,7 @@ struct SubArgs {
     const int *idisp;         /* [nchan], ascending frequency */
     long long nvalid;         /* samples with data: (nb - 1) * L */
     long long sfill;          /* samples written per subband */
-    uint16_t *sub;
+    uint32_t *sub;            /* S: [nsub][sstride] words (samples w, w + DM_P) */
     long long sstride;
     /* clipped runs (dd_subband_clip) */
     const uint8_t *flags;     /* [nflags] 1: spectrum replaced */
@@ -209,7 +271,10 @@ __global__ void __launch_bounds__(SB_THREADS) dd_subband_u8(const SubArgs a)
 #pragma unroll 8
             for (int k = 0; k < a.cps; k++) acc += base[co[k]];
         }
-        a.sub[(long long)(s0 + sl) * a.sstride + T] = (uint16_t)acc;
+        /* low half of word T, high half of word T - DM_P */
+        uint16_t *row = reinterpret_cast<uint16_t *>(a.sub + (long long)(s0 + sl) * a.sstride);
+        row[2 * T] = (uint16_t)acc;
+        if (T >= DM_P) row[2 * (T - DM_P) + 1] = (uint16_t)acc;
     }
 }
 
@@ -265,116 +330,196 @@ __global__ void __launch_bounds__(SB_THREADS) dd_subband_clip(const SubArgs a)
 /* DM stage                                                          */
 /* ---------------------------------------------------------------- */
 struct DmArgs {
-    const uint16_t *sub;
-    long long sstride;
-    int nsub, ndm;
+    const uint32_t *sub;      /* S: [nsub][sstride] words */
+    long long sstride;        /* words per subband row */
+    int nsub, nsub8, ndm;
     int G;                    /* DMs per group (<= DM_G) */
+    int ngroups;
     const int *offs;          /* [ndm][nsub] (direct kernel) */
     int flush;                /* subbands per packed-accumulator flush */
-    int flush8;               /* flush rounded down to 8 when nsub % 8 == 0, else 0 */
-    const long long *chunk;   /* [ngroups][maxch]: S element offset (from T0) of each staged
-                                 16-byte chunk */
-    const int *nch;           /* [ngroups]: chunks staged */
-    int maxch;
-    const int *code;          /* [ngroups][G][nsub]: shared word of the window pair
-                                 (the shifted copy at +smem_words for odd offsets) */
-    int smem_words;           /* staged words per CTA (largest group) */
+    const int4 *win;          /* [ngroups][nsub]: window start (words from the tile
+                                 start, a multiple of 4), its shared word, its words */
+    const uint16_t *code;     /* [ngroups][G][nsub8]: shared word of each (DM, subband)
+                                 row; padding subbands and absent DMs read the zero row */
+    const int *gbytes;        /* [ngroups]: bytes of the group's windows */
+    int code_bytes;           /* bytes of one group's code block (a multiple of 16) */
+    int code_word, zero_word; /* word offsets in a stage */
+    int stage_words, nstage;
+    long long nitems;         /* tiles x groups */
     long long nout;
     float *out;
     long long ostride;
+    int *err;                 /* set when a wait gave up */
 };
 
-__global__ void __launch_bounds__(DM_THREADS) dd_dms_u16(const DmArgs a)
+/* The integer DM stage, warp-specialised over a ring of nstage shared
+ * buffers.  Work item = (tile of DM_TILE samples, group of G consecutive
+ * DMs), the group index fastest; CTA b takes items b, b + grid, ... so the
+ * CTAs sweep the series together and the S rows they read stay in L2.
+ *   copy warp:     per item one bulk copy per subband window (the union of
+ *                  the group's DM windows, from a multiple of 4 words) and
+ *                  one of the group's code block, all completing on the
+ *                  stage's full barrier;
+ *   summing warps: warp w sums DMs w, w + NCW, ... of the group for the
+ *                  columns c = lane + 32 k: one shared word per (DM,
+ *                  subband, column) gives samples T0 + c and T0 + c + DM_P,
+ *                  added with one 32-bit add (two 16-bit lanes, widened
+ *                  every `flush` subbands before they can carry); lanes
+ *                  read consecutive words.  The stage is released before
+ *                  the float stores.
+ * Bound: shared-memory reads, 2 B per subband term. */
+__global__ void __launch_bounds__(DM_THREADS, 1) dd_dms_u16(const DmArgs a)
 {
-    /* shared: staged words [0, W) | the same rows shifted by one sample
-     * [W, 2W): word w there holds samples (2w+1, 2w+2) | (DM, subband) codes */
-    extern __shared__ __align__(16) uint32_t smw[];
-    const int g = blockIdx.x;                              /* DM group */
-    const long long T0 = (long long)blockIdx.y * DM_TT;
-    const int W = a.smem_words;
-    const int *code = a.code + (size_t)g * a.G * a.nsub;
-    int *code_s = reinterpret_cast<int *>(smw + 2 * W);
-
-    for (int i = threadIdx.x; i < a.G * a.nsub; i += blockDim.x) code_s[i] = code[i];
-    /* stage the group's windows (subband after subband, each from a multiple
-     * of 8 samples): 16-byte chunk i of shared memory comes from
-     * S + T0 + chunk[i] */
-    const long long *chunk = a.chunk + (size_t)g * a.maxch;
-    const int nch = a.nch[g];
-    const uint16_t *sub0 = a.sub + T0;
-    for (int i = threadIdx.x; i < nch; i += blockDim.x) cp_async16(smw + 4 * i, sub0 + chunk[i]);
-    cp_async_wait_all();
+    extern __shared__ __align__(128) uint32_t smw[];
+    __shared__ __align__(8) unsigned long long bars[2 * DM_MAXST];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t full0 = smem_addr(&bars[0]), empty0 = smem_addr(&bars[DM_MAXST]);
+    const int NS = a.nstage;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < NS; i++) {
+            mbar_init(full0 + 8 * i, 1);
+            mbar_init(empty0 + 8 * i, DM_NCW);
+        }
+        mbar_fence_init();
+    }
+    for (int st = 0; st < NS; st++)
+        for (int i = threadIdx.x; i < DM_P; i += blockDim.x)
+            smw[(size_t)st * a.stage_words + a.zero_word + i] = 0;
     __syncthreads();
-    /* the copy shifted by one sample (pairs straddling two windows are never read) */
-    for (int i = threadIdx.x; i + 1 < 4 * nch; i += blockDim.x)
-        smw[W + i] = __byte_perm(smw[i], smw[i + 1], 0x5432);
-    __syncthreads();
+    const long long grid = gridDim.x;
 
-    /* thread: sample pairs (2 tt + 2 (DM_TT / DM_R) j, +1), j < 4, of DM_GD
-     * DMs; a warp's lanes read consecutive words, so loads are conflict-free */
-    constexpr int NP = DM_R / 2;                           /* pairs per thread */
-    constexpr int PS = DM_TT / DM_R;                       /* pair stride */
-    const int tt = threadIdx.x % PS;
-    const int dq = threadIdx.x / PS;
-    const uint32_t *wt = smw + tt;
-    for (int dd = 0; dd < DM_GD; dd++) {
-        const int dl = dq + (DM_G / DM_GD) * dd;           /* DM within group */
-        const int d = g * a.G + dl;
-        if (dl >= a.G || d >= a.ndm) break;
-        uint32_t acc[DM_R];
+    if (warp == DM_NCW) {
+        /* ------------------------------ copy warp ------------------------------ */
+        long long k = 0;
+        bool ok = true;
+        for (long long item = blockIdx.x; item < a.nitems; item += grid, k++) {
+            const int st = (int)(k % NS);
+            const uint32_t ph = (uint32_t)(k / NS) & 1u;
+            if (k >= NS) ok = __all_sync(0xffffffffu, mbar_wait(empty0 + 8 * st, ph ^ 1u));
+            if (!ok) break;
+            const long long tile = item / a.ngroups;
+            const int g = (int)(item - tile * a.ngroups);
+            const uint32_t fb = full0 + 8 * st;
+            if (lane == 0) mbar_arrive_tx(fb, (uint32_t)(__ldg(a.gbytes + g) + a.code_bytes));
+            __syncwarp();
+            uint32_t *stage = smw + (size_t)st * a.stage_words;
+            const uint32_t *src0 = a.sub + tile * DM_TILE;
+            for (int s = lane; s < a.nsub; s += 32) {
+                const int4 w = __ldg(a.win + (size_t)g * a.nsub + s);
+                bulk_g2s(stage + w.y, src0 + (long long)s * a.sstride + w.x, (uint32_t)w.z * 4u, fb);
+            }
+            if (lane == 0)
+                bulk_g2s(stage + a.code_word, a.code + (size_t)g * a.G * a.nsub8,
+                         (uint32_t)a.code_bytes, fb);
+        }
+        if (!ok && lane == 0) atomicExch(a.err, 1);
+        /* never leave with copies in flight: the last use of each stage landed */
+        for (long long j = k > NS ? k - NS : 0; j < k; j++)
+            if (!mbar_wait(full0 + 8 * (int)(j % NS), (uint32_t)(j / NS) & 1u) && lane == 0)
+                atomicExch(a.err, 1);
+        return;
+    }
+
+    /* ---------------------------- summing warps ---------------------------- */
+    long long k = 0;
+    for (long long item = blockIdx.x; item < a.nitems; item += grid, k++) {
+        const int st = (int)(k % NS);
+        const uint32_t ph = (uint32_t)(k / NS) & 1u;
+        if (!__all_sync(0xffffffffu, mbar_wait(full0 + 8 * st, ph))) {
+            if (lane == 0) atomicExch(a.err, 1);
+            break;
+        }
+        const long long tile = item / a.ngroups;
+        const int g = (int)(item - tile * a.ngroups);
+        const uint32_t *stage = smw + (size_t)st * a.stage_words;
+        const uint16_t *cb = reinterpret_cast<const uint16_t *>(stage + a.code_word);
+        const uint32_t *col = stage + lane;
+        uint32_t lo[DM_DPT][DM_CPT], hi[DM_DPT][DM_CPT], p[DM_DPT][DM_CPT];
 #pragma unroll
-        for (int r = 0; r < DM_R; r++) acc[r] = 0;
-        const int *cd = code_s + dl * a.nsub;
-        if (a.flush8 > 0) {
-            /* 8 subbands per step: two vector loads of codes, then 32
-             * independent shared loads */
-            for (int sb = 0; sb < a.nsub; sb += a.flush8) {
-                uint32_t p[NP];
+        for (int j = 0; j < DM_DPT; j++)
 #pragma unroll
-                for (int k = 0; k < NP; k++) p[k] = 0;
-                const int se = min(sb + a.flush8, a.nsub);
-                for (int s = sb; s < se; s += 8) {
-                    const int4 ca = *reinterpret_cast<const int4 *>(cd + s);
-                    const int4 cb = *reinterpret_cast<const int4 *>(cd + s + 4);
-                    const int cc[8] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
+            for (int c = 0; c < DM_CPT; c++) lo[j][c] = hi[j][c] = p[j][c] = 0;
+        /* widen the packed sums every `flush` subbands: at 8-subband block
+         * boundaries when flush >= 8 (no branch among a block's loads) */
+        const int fl8 = a.flush >= 8 ? a.flush / 8 : 0;
+        int cnt = 0;
+        for (int s8 = 0; s8 < a.nsub8; s8 += 8) {
+            uint32_t cw[DM_DPT][4];
 #pragma unroll
-                    for (int u = 0; u < 8; u++)
-#pragma unroll
-                        for (int k = 0; k < NP; k++) p[k] += wt[cc[u] + k * PS];
-                }
-#pragma unroll
-                for (int k = 0; k < NP; k++) {
-                    acc[2 * k] += p[k] & 0xffffu;
-                    acc[2 * k + 1] += p[k] >> 16;
+            for (int j = 0; j < DM_DPT; j++) {
+                const int dl = warp + DM_NCW * j;
+                if (dl < a.G) {
+                    const uint4 v = *reinterpret_cast<const uint4 *>(cb + (size_t)dl * a.nsub8 + s8);
+                    cw[j][0] = v.x; cw[j][1] = v.y; cw[j][2] = v.z; cw[j][3] = v.w;
+                } else {
+                    const uint32_t z = (uint32_t)a.zero_word * 0x10001u;
+                    cw[j][0] = cw[j][1] = cw[j][2] = cw[j][3] = z;
                 }
             }
-        } else {
-            for (int sb = 0; sb < a.nsub; sb += a.flush) {
-                uint32_t p[NP];
+            if (fl8) {
 #pragma unroll
-                for (int k = 0; k < NP; k++) p[k] = 0;
-                const int se = min(sb + a.flush, a.nsub);
-                for (int s = sb; s < se; s++) {
-                    const int c = cd[s];
+                for (int u = 0; u < 8; u++)
 #pragma unroll
-                    for (int k = 0; k < NP; k++) p[k] += wt[c + k * PS];
+                    for (int j = 0; j < DM_DPT; j++) {
+                        const uint32_t off = (u & 1) ? (cw[j][u >> 1] >> 16) : (cw[j][u >> 1] & 0xffffu);
+#pragma unroll
+                        for (int c = 0; c < DM_CPT; c++) p[j][c] += col[off + 32 * c];
+                    }
+                if (++cnt == fl8) {
+                    cnt = 0;
+#pragma unroll
+                    for (int j = 0; j < DM_DPT; j++)
+#pragma unroll
+                        for (int c = 0; c < DM_CPT; c++) {
+                            lo[j][c] += p[j][c] & 0xffffu;
+                            hi[j][c] += p[j][c] >> 16;
+                            p[j][c] = 0;
+                        }
                 }
+            } else {
 #pragma unroll
-                for (int k = 0; k < NP; k++) {
-                    acc[2 * k] += p[k] & 0xffffu;
-                    acc[2 * k + 1] += p[k] >> 16;
+                for (int u = 0; u < 8; u++) {
+#pragma unroll
+                    for (int j = 0; j < DM_DPT; j++) {
+                        const uint32_t off = (u & 1) ? (cw[j][u >> 1] >> 16) : (cw[j][u >> 1] & 0xffffu);
+#pragma unroll
+                        for (int c = 0; c < DM_CPT; c++) p[j][c] += col[off + 32 * c];
+                    }
+                    if (++cnt == a.flush) {
+                        cnt = 0;
+#pragma unroll
+                        for (int j = 0; j < DM_DPT; j++)
+#pragma unroll
+                            for (int c = 0; c < DM_CPT; c++) {
+                                lo[j][c] += p[j][c] & 0xffffu;
+                                hi[j][c] += p[j][c] >> 16;
+                                p[j][c] = 0;
+                            }
+                    }
                 }
             }
         }
-        float *o = a.out + (long long)d * a.ostride + T0 + 2 * tt;
 #pragma unroll
-        for (int k = 0; k < NP; k++) {
-            const long long T = T0 + 2 * tt + 2 * PS * k;
-            float *ok = o + 2 * PS * k;
-            if (T + 2 <= a.nout) {
-                *reinterpret_cast<float2 *>(ok) = make_float2((float)acc[2 * k], (float)acc[2 * k + 1]);
-            } else if (T < a.nout) {
-                ok[0] = (float)acc[2 * k];
+        for (int j = 0; j < DM_DPT; j++)
+#pragma unroll
+            for (int c = 0; c < DM_CPT; c++) {
+                lo[j][c] += p[j][c] & 0xffffu;
+                hi[j][c] += p[j][c] >> 16;
+            }
+        /* the sums are in registers: release the stage, then store */
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty0 + 8 * st);
+        const long long T0 = tile * DM_TILE;
+#pragma unroll
+        for (int j = 0; j < DM_DPT; j++) {
+            const int dl = warp + DM_NCW * j;
+            const int d = g * a.G + dl;
+            if (dl >= a.G || d >= a.ndm) break;
+            float *o = a.out + (long long)d * a.ostride + T0 + lane;
+#pragma unroll
+            for (int c = 0; c < DM_CPT; c++) {
+                if (T0 + lane + 32 * c < a.nout) o[32 * c] = (float)lo[j][c];
+                if (T0 + DM_P + lane + 32 * c < a.nout) o[DM_P + 32 * c] = (float)hi[j][c];
             }
         }
     }
@@ -388,8 +533,10 @@ __global__ void __launch_bounds__(256) dd_dms_u16_direct(const DmArgs a)
     const int d = blockIdx.y;
     if (T >= a.nout) return;
     const int *off = a.offs + (size_t)d * a.nsub;
+    const uint16_t *s16 = reinterpret_cast<const uint16_t *>(a.sub);
     uint32_t acc = 0;
-    for (int s = 0; s < a.nsub; s++) acc += __ldg(a.sub + (long long)s * a.sstride + T + off[s]);
+    /* sample x of a subband row is the low half of its word x */
+    for (int s = 0; s < a.nsub; s++) acc += __ldg(s16 + 2 * ((long long)s * a.sstride + T + off[s]));
     a.out[(long long)d * a.ostride + T] = (float)acc;
 }
 
@@ -500,6 +647,157 @@ __global__ void __launch_bounds__(256, 3) dd_dms_f32(const float *subf, long lon
     }
 }
 
+/* The DM stage of a clipped run, warp-specialised like dd_dms_u16: work
+ * item = (tile of FD_T samples, group of G consecutive DMs), the group index
+ * fastest, CTA b taking items b, b + grid, ...; a copy warp bulk-copies the
+ * item's subband windows (floats, from a multiple of 4) and its code block
+ * into a ring of stages; summing warp w adds, for DMs w, w + NCW, ... of the
+ * group, the subbands in ascending order from -0.0f for the samples
+ * lane + 32 k (FP32, the reference's order: dispersion.c:346-362).  S is
+ * filled up to sfill samples; every written output reads below it. */
+constexpr int FD_T = 256;                 /* samples per tile */
+constexpr int FD_NCW = 16;                /* summing warps */
+constexpr int FD_SPL = FD_T / 32;         /* samples a lane */
+constexpr int FD_DPW = DM_G / FD_NCW;     /* most DMs a summing warp */
+constexpr int FD_THREADS = (FD_NCW + 1) * 32;
+
+struct FdArgs {
+    const float *sub;         /* S: [nsub][sstride] floats */
+    long long sstride;
+    int nsub, nsub8, ndm, G, ngroups;
+    const int4 *win;          /* [ngroups][nsub]: window start (floats from the tile start,
+                                 a multiple of 4), its stage float, its floats */
+    const uint16_t *code;     /* [ngroups][G][nsub8]: stage float of each (DM, subband) row */
+    const int *gbytes;        /* [ngroups]: bytes of the group's windows */
+    int code_bytes, code_word, stage_words, nstage;
+    long long nitems;
+    long long nout;
+    float *out;
+    long long ostride;
+    int *err;
+};
+
+__global__ void __launch_bounds__(FD_THREADS, 1) dd_dms_f32_ws(const FdArgs a)
+{
+    extern __shared__ __align__(128) float smf[];
+    __shared__ __align__(8) unsigned long long bars[2 * DM_MAXST];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t full0 = smem_addr(&bars[0]), empty0 = smem_addr(&bars[DM_MAXST]);
+    const int NS = a.nstage;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < NS; i++) {
+            mbar_init(full0 + 8 * i, 1);
+            mbar_init(empty0 + 8 * i, FD_NCW);
+        }
+        mbar_fence_init();
+    }
+    __syncthreads();
+    const long long grid = gridDim.x;
+
+    if (warp == FD_NCW) {
+        /* ------------------------------ copy warp ------------------------------ */
+        long long k = 0;
+        bool ok = true;
+        for (long long item = blockIdx.x; item < a.nitems; item += grid, k++) {
+            const int st = (int)(k % NS);
+            const uint32_t ph = (uint32_t)(k / NS) & 1u;
+            if (k >= NS) ok = __all_sync(0xffffffffu, mbar_wait(empty0 + 8 * st, ph ^ 1u));
+            if (!ok) break;
+            const long long tile = item / a.ngroups;
+            const int g = (int)(item - tile * a.ngroups);
+            const uint32_t fb = full0 + 8 * st;
+            if (lane == 0) mbar_arrive_tx(fb, (uint32_t)(__ldg(a.gbytes + g) + a.code_bytes));
+            __syncwarp();
+            float *stage = smf + (size_t)st * a.stage_words;
+            const float *src0 = a.sub + tile * FD_T;
+            for (int s = lane; s < a.nsub; s += 32) {
+                const int4 w = __ldg(a.win + (size_t)g * a.nsub + s);
+                bulk_g2s(stage + w.y, src0 + (long long)s * a.sstride + w.x, (uint32_t)w.z * 4u, fb);
+            }
+            if (lane == 0)
+                bulk_g2s(stage + a.code_word, a.code + (size_t)g * a.G * a.nsub8,
+                         (uint32_t)a.code_bytes, fb);
+        }
+        if (!ok && lane == 0) atomicExch(a.err, 1);
+        for (long long j = k > NS ? k - NS : 0; j < k; j++)
+            if (!mbar_wait(full0 + 8 * (int)(j % NS), (uint32_t)(j / NS) & 1u) && lane == 0)
+                atomicExch(a.err, 1);
+        return;
+    }
+
+    /* ---------------------------- summing warps ---------------------------- */
+    long long k = 0;
+    for (long long item = blockIdx.x; item < a.nitems; item += grid, k++) {
+        const int st = (int)(k % NS);
+        const uint32_t ph = (uint32_t)(k / NS) & 1u;
+        if (!__all_sync(0xffffffffu, mbar_wait(full0 + 8 * st, ph))) {
+            if (lane == 0) atomicExch(a.err, 1);
+            break;
+        }
+        const long long tile = item / a.ngroups;
+        const int g = (int)(item - tile * a.ngroups);
+        const float *stage = smf + (size_t)st * a.stage_words;
+        const uint16_t *cb = reinterpret_cast<const uint16_t *>(stage + a.code_word);
+        const float *col = stage + lane;
+        float acc[FD_DPW][FD_SPL];
+#pragma unroll
+        for (int j = 0; j < FD_DPW; j++)
+#pragma unroll
+            for (int q = 0; q < FD_SPL; q++) acc[j][q] = -0.0f;
+        /* this warp's DMs of the group (warp-uniform) */
+        int ndw = 0;
+#pragma unroll
+        for (int j = 0; j < FD_DPW; j++)
+            if (warp + FD_NCW * j < a.G) ndw = j + 1;
+        for (int s8 = 0; s8 < a.nsub8; s8 += 8) {
+            uint32_t cw[FD_DPW][4];
+#pragma unroll
+            for (int j = 0; j < FD_DPW; j++) {
+                const int dl = min(warp + FD_NCW * j, a.G - 1);
+                const uint4 v = *reinterpret_cast<const uint4 *>(cb + (size_t)dl * a.nsub8 + s8);
+                cw[j][0] = v.x; cw[j][1] = v.y; cw[j][2] = v.z; cw[j][3] = v.w;
+            }
+            if (s8 + 8 <= a.nsub) {
+#pragma unroll
+                for (int u = 0; u < 8; u++)
+#pragma unroll
+                    for (int j = 0; j < FD_DPW; j++) {
+                        if (j >= ndw) break;
+                        const uint32_t off = (u & 1) ? (cw[j][u >> 1] >> 16) : (cw[j][u >> 1] & 0xffffu);
+#pragma unroll
+                        for (int q = 0; q < FD_SPL; q++)
+                            acc[j][q] = __fadd_rn(acc[j][q], col[off + 32 * q]);
+                    }
+            } else {
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    if (s8 + u >= a.nsub) break;
+#pragma unroll
+                    for (int j = 0; j < FD_DPW; j++) {
+                        if (j >= ndw) break;
+                        const uint32_t off = (u & 1) ? (cw[j][u >> 1] >> 16) : (cw[j][u >> 1] & 0xffffu);
+#pragma unroll
+                        for (int q = 0; q < FD_SPL; q++)
+                            acc[j][q] = __fadd_rn(acc[j][q], col[off + 32 * q]);
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty0 + 8 * st);
+        const long long T0 = tile * FD_T;
+#pragma unroll
+        for (int j = 0; j < FD_DPW; j++) {
+            const int d = g * a.G + warp + FD_NCW * j;
+            if (j >= ndw || d >= a.ndm) break;
+            float *o = a.out + (long long)d * a.ostride + T0 + lane;
+#pragma unroll
+            for (int q = 0; q < FD_SPL; q++)
+                if (T0 + lane + 32 * q < a.nout) o[32 * q] = acc[j][q];
+        }
+    }
+}
+
 }  // namespace dd
 
 /* ---------------------------------------------------------------- */
@@ -511,18 +809,25 @@ struct CsDedisp {
     long long max_spectra;
     int halo, maxoff;
     int flush;
-    int G;                         /* DMs per staged group; 0: direct kernel */
+    int G;                         /* DMs per group of the DM stage; 0: direct kernel */
     int ngroups;
-    int smem_words;
-    int maxch = 0;
+    int nsub8, code_bytes, code_word, zero_word, stage_words, nstage;
     int *d_idisp = nullptr;
     int *d_offs = nullptr;
-    int *d_code = nullptr, *d_nch = nullptr;
-    long long *d_chunk = nullptr;
-    uint16_t *d_sub = nullptr;
+    int4 *d_win = nullptr;
+    uint16_t *d_code = nullptr;
+    int *d_gbytes = nullptr;
+    int *d_err = nullptr;          /* set by a DM-stage wait that gave up */
+    uint32_t *d_sub = nullptr;
     float *d_subf = nullptr;       /* S of clipped runs (allocated by the first one) */
-    int2 *d_fwin = nullptr;        /* clipped DM stage: per (DM group, subband) window */
+    int2 *d_fwin = nullptr;        /* clipped DM stage (rounds kernel): per (DM group, subband)
+                                      window */
     int fwmax = 0;                 /* widest such window (floats) */
+    /* clipped DM stage, warp-specialised kernel (fG 0: the rounds kernel) */
+    int fG = 0, fngroups = 0, fcode_bytes = 0, fcode_word = 0, fstage_words = 0, fnstage = 0;
+    int4 *d_fwin2 = nullptr;
+    uint16_t *d_fcode = nullptr;
+    int *d_fgbytes = nullptr;
     long long sstride = 0;
     uint8_t *d_raw = nullptr;      /* staging for the host-memory entry point */
     float *d_out = nullptr;
@@ -537,11 +842,15 @@ static void dd_release(CsDedisp *D)
     cudaFree(D->d_idisp);
     cudaFree(D->d_offs);
     cudaFree(D->d_code);
-    cudaFree(D->d_nch);
-    cudaFree(D->d_chunk);
+    cudaFree(D->d_win);
+    cudaFree(D->d_gbytes);
+    cudaFree(D->d_err);
     cudaFree(D->d_sub);
     cudaFree(D->d_subf);
     cudaFree(D->d_fwin);
+    cudaFree(D->d_fwin2);
+    cudaFree(D->d_fcode);
+    cudaFree(D->d_fgbytes);
     cudaFree(D->d_raw);
     cudaFree(D->d_out);
     if (D->st) cudaStreamDestroy(D->st);
@@ -694,19 +1003,25 @@ CS_EXPORT CsDedisp *cs_dedisp_create(int nchan, int nsub, int ndm, const int *id
         return nullptr;
     }
     /* DM-stage tables for groups of G consecutive DMs: per (group, subband)
-     * the window start (a multiple of 8 samples), its word base in shared
-     * memory and its word count (multiples of 4); per (DM, subband) the word
-     * offset and parity.  G is the largest of 32, 16, ..., 1 whose windows fit
-     * in shared memory; 0 selects the direct kernel. */
+     * the window (from the group's lowest offset rounded down to 4 words, up
+     * to its highest offset + DM_P, rounded up to 4 words) and its word in a
+     * stage; per (group, DM, subband) the stage word of the DM's row.  A
+     * stage holds the windows, the group's code block and a zero row.  G is
+     * the largest of 32, 16, ..., 1 whose stages fit twice in shared memory;
+     * 0 selects the direct kernel. */
     int max_optin = 0;
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
-    std::vector<int> win, code;
-    int G = dd::DM_G, smem_words = 0;
+    const int nsub8 = (nsub + 7) / 8 * 8;
+    std::vector<int4> win;
+    std::vector<uint16_t> code;
+    std::vector<int> gbytes;
+    /* CS_B200_DEDISP_DIRECT=1 selects the direct kernel (its tests) */
+    int G = getenv("CS_B200_DEDISP_DIRECT") ? 0 : dd::DM_G;
     for (; G >= 1; G /= 2) {
         const int ngroups = (ndm + G - 1) / G;
-        win.assign((size_t)ngroups * nsub * 3, 0);
-        code.assign((size_t)ngroups * G * nsub, 0);
-        smem_words = 0;
+        win.assign((size_t)ngroups * nsub, make_int4(0, 0, 0, 0));
+        gbytes.assign(ngroups, 0);
+        int wmax = 0;
         for (int g = 0; g < ngroups; g++) {
             int wb = 0;
             for (int s = 0; s < nsub; s++) {
@@ -715,56 +1030,93 @@ CS_EXPORT CsDedisp *cs_dedisp_create(int nchan, int nsub, int ndm, const int *id
                     omin = std::min(omin, offsets[(size_t)(g * G + dl) * nsub + s]);
                     omax = std::max(omax, offsets[(size_t)(g * G + dl) * nsub + s]);
                 }
-                const int start = omin & ~7;
-                const int words = ((dd::DM_TT + (omax - start) + 3) / 2 + 3) / 4 * 4;
-                win[((size_t)g * nsub + s) * 3] = start;
-                win[((size_t)g * nsub + s) * 3 + 1] = wb;
-                win[((size_t)g * nsub + s) * 3 + 2] = words;
-                for (int dl = 0; dl < G && g * G + dl < ndm; dl++) {
-                    const int rel = offsets[(size_t)(g * G + dl) * nsub + s] - start;
-                    code[((size_t)g * G + dl) * nsub + s] = ((wb + (rel >> 1)) << 1) | (rel & 1);
-                }
+                const int start = omin & ~3;
+                const int words = (omax - start + dd::DM_P + 3) / 4 * 4;
+                win[(size_t)g * nsub + s] = make_int4(start, wb, words, 0);
                 wb += words;
             }
-            smem_words = std::max(smem_words, wb);
+            gbytes[g] = 4 * wb;
+            wmax = std::max(wmax, wb);
         }
-        if ((long long)smem_words * 8 + (long long)G * nsub * 4 <= max_optin) break;
+        D->code_bytes = 2 * G * nsub8;                  /* a multiple of 16 */
+        D->code_word = wmax;                            /* a multiple of 4 */
+        D->zero_word = wmax + D->code_bytes / 4;
+        D->stage_words = (D->zero_word + dd::DM_P + 31) / 32 * 32;
+        const long long room = (long long)max_optin - 1024;   /* static barriers */
+        D->nstage = (int)std::min<long long>(dd::DM_MAXST, room / (4LL * D->stage_words));
+        if (D->nstage >= 2 && D->zero_word < 65536) break;
     }
-    /* codes -> absolute shared words: odd offsets read the shifted copy */
-    for (int &c : code) c = (c >> 1) + ((c & 1) ? smem_words : 0);
-    D->G = G;
+    D->G = std::max(G, 0);
     D->ngroups = G > 0 ? (ndm + G - 1) / G : 0;
-    D->smem_words = G > 0 ? smem_words : 0;
-    const size_t dm_smem = G > 0 ? (size_t)smem_words * 8 + (size_t)G * nsub * 4 : 0;
+    D->nsub8 = nsub8;
+    if (G > 0) {
+        code.assign((size_t)D->ngroups * G * nsub8, (uint16_t)D->zero_word);
+        for (int g = 0; g < D->ngroups; g++)
+            for (int dl = 0; dl < G && g * G + dl < ndm; dl++)
+                for (int s = 0; s < nsub; s++) {
+                    const int4 w = win[(size_t)g * nsub + s];
+                    const int rel = offsets[(size_t)(g * G + dl) * nsub + s] - w.x;
+                    code[((size_t)g * G + dl) * nsub8 + s] = (uint16_t)(w.y + rel);
+                }
+    }
+    /* the clipped DM stage's tables: as above with float windows of
+     * FD_T + the group's offset spread (the warp-specialised kernel), for
+     * the largest G of 32, 16, ..., 1 whose stages fit twice */
+    std::vector<int4> fwin2;
+    std::vector<uint16_t> fcode;
+    std::vector<int> fgbytes;
+    {
+        int FGs = dd::DM_G;
+        for (; FGs >= 1; FGs /= 2) {
+            const int ng = (ndm + FGs - 1) / FGs;
+            fwin2.assign((size_t)ng * nsub, make_int4(0, 0, 0, 0));
+            fgbytes.assign(ng, 0);
+            int wmax = 0;
+            for (int g = 0; g < ng; g++) {
+                int wb = 0;
+                for (int s = 0; s < nsub; s++) {
+                    int omin = 1 << 30, omax = 0;
+                    for (int dl = 0; dl < FGs && g * FGs + dl < ndm; dl++) {
+                        omin = std::min(omin, offsets[(size_t)(g * FGs + dl) * nsub + s]);
+                        omax = std::max(omax, offsets[(size_t)(g * FGs + dl) * nsub + s]);
+                    }
+                    const int start = omin & ~3;
+                    const int n = (omax - start + dd::FD_T + 3) / 4 * 4;
+                    fwin2[(size_t)g * nsub + s] = make_int4(start, wb, n, 0);
+                    wb += n;
+                }
+                fgbytes[g] = 4 * wb;
+                wmax = std::max(wmax, wb);
+            }
+            D->fcode_bytes = 2 * FGs * nsub8;
+            D->fcode_word = wmax;
+            D->fstage_words = (wmax + D->fcode_bytes / 4 + 31) / 32 * 32;
+            const long long room = (long long)max_optin - 1024;
+            D->fnstage = (int)std::min<long long>(dd::DM_MAXST, room / (4LL * D->fstage_words));
+            if (D->fnstage >= 2 && D->fcode_word < 65536) break;
+        }
+        D->fG = std::max(FGs, 0);
+        D->fngroups = D->fG > 0 ? (ndm + D->fG - 1) / D->fG : 0;
+        if (D->fG > 0) {
+            fcode.assign((size_t)D->fngroups * D->fG * nsub8, 0);
+            for (int g = 0; g < D->fngroups; g++)
+                for (int dl = 0; dl < D->fG && g * D->fG + dl < ndm; dl++)
+                    for (int s = 0; s < nsub; s++) {
+                        const int4 w = fwin2[(size_t)g * nsub + s];
+                        const int rel = offsets[(size_t)(g * D->fG + dl) * nsub + s] - w.x;
+                        fcode[((size_t)g * D->fG + dl) * nsub8 + s] = (uint16_t)(w.y + rel);
+                    }
+        }
+    }
     if (sb_smem(D, 1) > max_optin) {
         fprintf(stderr, "Error: cs_dedisp_create: channel delays of %d samples need more "
                         "shared memory than a CTA has\n", halo);
         dd_release(D);
         return nullptr;
     }
-    /* staging chunks: per group, the windows in subband order; the subband
-     * index rides in the high bits until the row stride is known */
-    std::vector<long long> chunks;
-    std::vector<int> nch;
-    if (G > 0) {
-        D->maxch = smem_words / 4;
-        chunks.assign((size_t)D->ngroups * D->maxch, 0);
-        nch.assign(D->ngroups, 0);
-        for (int g = 0; g < D->ngroups; g++) {
-            int n = 0;
-            for (int s = 0; s < nsub; s++) {
-                const int start = win[((size_t)g * nsub + s) * 3];
-                const int words = win[((size_t)g * nsub + s) * 3 + 2];
-                for (int j = 0; j < words / 4; j++)
-                    chunks[(size_t)g * D->maxch + n++] = ((long long)s << 40) + start + 8LL * j;
-            }
-            nch[g] = n;
-        }
-    }
-    /* S is read up to (tiles * DM_TT) + maxoff + a few words beyond */
-    const long long ntile = (max_spectra + dd::DM_TT - 1) / dd::DM_TT;
-    D->sstride = ((ntile + 1) * dd::DM_TT + maxoff + 64 + 255) / 256 * 256;
-    for (long long &c : chunks) c = (c >> 40) * D->sstride + (c & ((1LL << 40) - 1));
+    /* S is read up to (tiles * DM_TILE) + maxoff + a few words beyond */
+    const long long ntile = (max_spectra + dd::DM_TILE - 1) / dd::DM_TILE;
+    D->sstride = ((ntile + 1) * dd::DM_TILE + maxoff + 64 + 255) / 256 * 256;
 #define DDCK(x)                                                                       \
     do {                                                                              \
         cudaError_t e_ = (x);                                                         \
@@ -779,15 +1131,34 @@ CS_EXPORT CsDedisp *cs_dedisp_create(int nchan, int nsub, int ndm, const int *id
     DDCK(cudaMalloc((void **)&D->d_offs, sizeof(int) * (size_t)ndm * nsub));
     DDCK(cudaMemcpy(D->d_offs, offsets, sizeof(int) * (size_t)ndm * nsub, cudaMemcpyHostToDevice));
     if (G > 0) {
-        DDCK(cudaMalloc((void **)&D->d_code, sizeof(int) * code.size()));
-        DDCK(cudaMemcpy(D->d_code, code.data(), sizeof(int) * code.size(), cudaMemcpyHostToDevice));
-        DDCK(cudaMalloc((void **)&D->d_chunk, sizeof(long long) * chunks.size()));
-        DDCK(cudaMemcpy(D->d_chunk, chunks.data(), sizeof(long long) * chunks.size(),
+        DDCK(cudaMalloc((void **)&D->d_code, sizeof(uint16_t) * code.size()));
+        DDCK(cudaMemcpy(D->d_code, code.data(), sizeof(uint16_t) * code.size(),
                         cudaMemcpyHostToDevice));
-        DDCK(cudaMalloc((void **)&D->d_nch, sizeof(int) * nch.size()));
-        DDCK(cudaMemcpy(D->d_nch, nch.data(), sizeof(int) * nch.size(), cudaMemcpyHostToDevice));
+        DDCK(cudaMalloc((void **)&D->d_win, sizeof(int4) * win.size()));
+        DDCK(cudaMemcpy(D->d_win, win.data(), sizeof(int4) * win.size(), cudaMemcpyHostToDevice));
+        DDCK(cudaMalloc((void **)&D->d_gbytes, sizeof(int) * gbytes.size()));
+        DDCK(cudaMemcpy(D->d_gbytes, gbytes.data(), sizeof(int) * gbytes.size(),
+                        cudaMemcpyHostToDevice));
     }
-    DDCK(cudaMalloc((void **)&D->d_sub, sizeof(uint16_t) * (size_t)nsub * D->sstride));
+    if (D->fG > 0) {
+        DDCK(cudaMalloc((void **)&D->d_fcode, sizeof(uint16_t) * fcode.size()));
+        DDCK(cudaMemcpy(D->d_fcode, fcode.data(), sizeof(uint16_t) * fcode.size(),
+                        cudaMemcpyHostToDevice));
+        DDCK(cudaMalloc((void **)&D->d_fwin2, sizeof(int4) * fwin2.size()));
+        DDCK(cudaMemcpy(D->d_fwin2, fwin2.data(), sizeof(int4) * fwin2.size(),
+                        cudaMemcpyHostToDevice));
+        DDCK(cudaMalloc((void **)&D->d_fgbytes, sizeof(int) * fgbytes.size()));
+        DDCK(cudaMemcpy(D->d_fgbytes, fgbytes.data(), sizeof(int) * fgbytes.size(),
+                        cudaMemcpyHostToDevice));
+        DDCK(cudaFuncSetAttribute(dd::dd_dms_f32_ws, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  4 * D->fnstage * D->fstage_words));
+    }
+    DDCK(cudaMalloc((void **)&D->d_err, sizeof(int)));
+    DDCK(cudaMemset(D->d_err, 0, sizeof(int)));
+    /* S: word w of a row holds samples w and w + DM_P; cleared once, so the
+     * high halves past the filled samples are zeros rather than stale bytes */
+    DDCK(cudaMalloc((void **)&D->d_sub, sizeof(uint32_t) * (size_t)nsub * D->sstride));
+    DDCK(cudaMemset(D->d_sub, 0, sizeof(uint32_t) * (size_t)nsub * D->sstride));
     {
         /* clipped DM stage: the union window of each group of FG DMs per subband */
         const int ng = (ndm + dd::FG - 1) / dd::FG;
@@ -815,7 +1186,7 @@ CS_EXPORT CsDedisp *cs_dedisp_create(int nchan, int nsub, int ndm, const int *id
     DDCK(cudaEventCreate(&D->ev2));
     if (G > 0)
         DDCK(cudaFuncSetAttribute(dd::dd_dms_u16, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)dm_smem));
+                                  4 * D->nstage * D->stage_words));
     DDCK(cudaFuncSetAttribute(dd::dd_subband_u8, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               max_optin));
     DDCK(cudaFuncSetAttribute(dd::dd_subband_clip, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -854,8 +1225,8 @@ static cudaError_t dd_enqueue(CsDedisp *D, const uint8_t *d_raw, long long nspec
     const bool clip = d_flags != nullptr;
     if (nout <= 0) return cudaSuccess;
     /* subband stage over every sample the DM stage can read */
-    const long long ntile_dm = (nout + dd::DM_TT - 1) / dd::DM_TT;
-    const long long sfill = std::min(D->sstride, ntile_dm * dd::DM_TT + D->maxoff + 64);
+    const long long ntile_dm = (nout + dd::DM_TILE - 1) / dd::DM_TILE;
+    const long long sfill = std::min(D->sstride, ntile_dm * dd::DM_TILE + D->maxoff + 64);
     int max_optin = 0;
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, D->device);
     int slab = std::max(1, std::min(D->nsub, 256 / std::max(1, D->cps)));
@@ -882,13 +1253,45 @@ static cudaError_t dd_enqueue(CsDedisp *D, const uint8_t *d_raw, long long nspec
     sa.flag_off = sb_flag_offset(D, slab);
     sa.subf = D->d_subf;
     dim3 gs((D->nsub + slab - 1) / slab, (unsigned)((sfill + dd::SB_TT - 1) / dd::SB_TT));
+    cudaError_t e = cudaMemsetAsync(D->d_err, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
     cudaEventRecord(D->ev0, st);
     if (clip)
         dd::dd_subband_clip<<<gs, dd::SB_THREADS, sb_smem(D, slab, true), st>>>(sa);
     else
         dd::dd_subband_u8<<<gs, dd::SB_THREADS, sb_smem(D, slab), st>>>(sa);
-    cudaError_t e = cudaGetLastError();
+    e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    if (clip && D->fG > 0 && !getenv("CS_B200_DEDISP_ROUNDS")) {
+        dd::FdArgs fa;
+        memset(&fa, 0, sizeof(fa));
+        fa.sub = D->d_subf;
+        fa.sstride = D->sstride;
+        fa.nsub = D->nsub;
+        fa.nsub8 = D->nsub8;
+        fa.ndm = D->ndm;
+        fa.G = D->fG;
+        fa.ngroups = D->fngroups;
+        fa.win = D->d_fwin2;
+        fa.code = D->d_fcode;
+        fa.gbytes = D->d_fgbytes;
+        fa.code_bytes = D->fcode_bytes;
+        fa.code_word = D->fcode_word;
+        fa.stage_words = D->fstage_words;
+        fa.nstage = D->fnstage;
+        fa.nitems = (nout + dd::FD_T - 1) / dd::FD_T * D->fngroups;
+        fa.nout = nout;
+        fa.out = d_out;
+        fa.ostride = ostride;
+        fa.err = D->d_err;
+        int nsm = 0;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, D->device);
+        const long long grid = std::min<long long>(fa.nitems, nsm);
+        cudaEventRecord(D->ev1, st);
+        dd::dd_dms_f32_ws<<<(unsigned)grid, dd::FD_THREADS, 4 * D->fnstage * D->fstage_words, st>>>(fa);
+        cudaEventRecord(D->ev2, st);
+        return cudaGetLastError();
+    }
     if (clip) {
         const long long ntile = (nout + dd::FT - 1) / dd::FT;
         const long long ngrp = (D->ndm + dd::FG - 1) / dd::FG;
@@ -901,33 +1304,58 @@ static cudaError_t dd_enqueue(CsDedisp *D, const uint8_t *d_raw, long long nspec
         return cudaGetLastError();
     }
     dd::DmArgs da;
+    memset(&da, 0, sizeof(da));
     da.sub = D->d_sub;
     da.sstride = D->sstride;
     da.nsub = D->nsub;
+    da.nsub8 = D->nsub8;
     da.ndm = D->ndm;
     da.G = D->G;
+    da.ngroups = D->ngroups;
     da.offs = D->d_offs;
     da.flush = D->flush;
-    da.flush8 = (D->nsub % 8 == 0 && D->flush >= 8) ? D->flush / 8 * 8 : 0;
-    da.chunk = D->d_chunk;
-    da.nch = D->d_nch;
-    da.maxch = D->maxch;
+    da.win = D->d_win;
     da.code = D->d_code;
-    da.smem_words = D->smem_words;
+    da.gbytes = D->d_gbytes;
+    da.code_bytes = D->code_bytes;
+    da.code_word = D->code_word;
+    da.zero_word = D->zero_word;
+    da.stage_words = D->stage_words;
+    da.nstage = D->nstage;
+    da.nitems = ntile_dm * D->ngroups;
     da.nout = nout;
     da.out = d_out;
     da.ostride = ostride;
+    da.err = D->d_err;
     cudaEventRecord(D->ev1, st);
     if (D->G > 0) {
-        const size_t dm_smem = (size_t)D->smem_words * 8 + (size_t)D->G * D->nsub * 4;
-        dim3 gd((unsigned)D->ngroups, (unsigned)ntile_dm);
-        dd::dd_dms_u16<<<gd, dd::DM_THREADS, dm_smem, st>>>(da);
+        int nsm = 0;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, D->device);
+        const long long grid = std::min<long long>(da.nitems, nsm);
+        dd::dd_dms_u16<<<(unsigned)grid, dd::DM_THREADS, 4 * D->nstage * D->stage_words, st>>>(da);
     } else {
         dim3 gd((unsigned)((nout + 255) / 256), (unsigned)D->ndm);
         dd::dd_dms_u16_direct<<<gd, 256, 0, st>>>(da);
     }
     cudaEventRecord(D->ev2, st);
     return cudaGetLastError();
+}
+
+/* 0, or -1 (with a message) if a wait of the last DM stage gave up; waits
+ * for the stream's work first. */
+static int dd_check(CsDedisp *D, cudaStream_t st, const char *who)
+{
+    int flag = 0;
+    if (cudaMemcpyAsync(&flag, D->d_err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        fprintf(stderr, "Error: %s: %s\n", who, cudaGetErrorString(cudaGetLastError()));
+        return -1;
+    }
+    if (flag) {
+        fprintf(stderr, "Error: %s: a DM-stage wait gave up (pipeline stalled)\n", who);
+        return -1;
+    }
+    return 0;
 }
 
 CS_EXPORT int cs_dedisp_run_device(CsDedisp *D, const uint8_t *d_raw, long long nspec,
@@ -977,13 +1405,16 @@ CS_EXPORT int cs_dedisp_run_device_clipped(CsDedisp *D, const uint8_t *d_raw, lo
                         "multiple of 4, the output 16-byte aligned\n", nout);
         return -1;
     }
-    if ((unsigned long long)((nout + dd::FT - 1) / dd::FT) *
-            (unsigned long long)((D->ndm + dd::FG - 1) / dd::FG) >= (1ULL << 31)) {
+    /* the rounds kernel (geometries whose windows the warp-specialised one
+     * cannot stage twice) has its limits */
+    const bool rounds = D->fG == 0 || getenv("CS_B200_DEDISP_ROUNDS");
+    if (rounds && (unsigned long long)((nout + dd::FT - 1) / dd::FT) *
+                          (unsigned long long)((D->ndm + dd::FG - 1) / dd::FG) >= (1ULL << 31)) {
         fprintf(stderr, "Error: cs_dedisp_run_device_clipped: %lld points x %d DMs is too many "
                         "for one launch\n", nout, D->ndm);
         return -1;
     }
-    if (dd_clip_rounds(D) < 1) {
+    if (rounds && dd_clip_rounds(D) < 1) {
         fprintf(stderr, "Error: cs_dedisp_run_device_clipped: subband windows of %d samples "
                         "(%d subbands) need more shared memory than a CTA has\n", D->fwmax,
                 D->nsub);
@@ -991,8 +1422,12 @@ CS_EXPORT int cs_dedisp_run_device_clipped(CsDedisp *D, const uint8_t *d_raw, lo
     }
     if (cudaSetDevice(D->device) != cudaSuccess) return -1;
     cudaError_t e = cudaSuccess;
-    if (!D->d_subf)
+    if (!D->d_subf) {
+        /* cleared once: staged samples past the filled ones are zeros */
         e = cudaMalloc((void **)&D->d_subf, sizeof(float) * (size_t)D->nsub * D->sstride);
+        if (e == cudaSuccess)
+            e = cudaMemset(D->d_subf, 0, sizeof(float) * (size_t)D->nsub * D->sstride);
+    }
     cudaStream_t st = stream ? (cudaStream_t)stream : D->st;
     if (e == cudaSuccess) e = dd_enqueue(D, d_raw, nspec, nout, d_out, out_stride, st, d_flags,
                                          d_levels);
@@ -1041,6 +1476,7 @@ CS_EXPORT int cs_dedisp_run(CsDedisp *D, const uint8_t *h_raw, long long nspec, 
         fprintf(stderr, "Error: cs_dedisp_run: %s\n", cudaGetErrorString(e));
         return -1;
     }
+    if (dd_check(D, D->st, "cs_dedisp_run") != 0) return -1;
     if (nout_written) *nout_written = nout;
     return 0;
 }
@@ -1051,6 +1487,7 @@ CS_EXPORT int cs_dedisp_last_times(CsDedisp *D, float *subband_ms, float *dm_ms)
 {
     if (!D) return -1;
     if (cudaEventSynchronize(D->ev2) != cudaSuccess) return -1;
+    if (dd_check(D, D->st, "cs_dedisp_last_times") != 0) return -1;
     float a = 0.0f, b = 0.0f;
     if (cudaEventElapsedTime(&a, D->ev0, D->ev1) != cudaSuccess ||
         cudaEventElapsedTime(&b, D->ev1, D->ev2) != cudaSuccess) {

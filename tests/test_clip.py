@@ -107,10 +107,18 @@ def _device_clipped(dd, t, raw, clip=6.0, numout=-1):
                                                  ("c64_s64_d7", 30, -1),
                                                  ("filterbank_1024x64x500", 8, -1),
                                                  ("c256_s16_d40", 40, 9000)])
-def test_clipped_dedispersion_matches_reference(gpu_ready, geom, nblocks, numout):
+@pytest.mark.parametrize("kernel", ["ws", "rounds"])
+def test_clipped_dedispersion_matches_reference(gpu_ready, monkeypatch, geom, nblocks, numout,
+                                                kernel):
     """prepsubband -clip on the GPU: the replaced spectra, the channel levels
     written over them (clip_times' good_chan_levels after every block) and the
-    dedispersed series, all bit for bit against the reference's own run."""
+    dedispersed series, all bit for bit against the reference's own run --
+    through the warp-specialised DM stage and through the rounds kernel it
+    falls back to (CS_B200_DEDISP_ROUNDS)."""
+    if kernel == "rounds":
+        monkeypatch.setenv("CS_B200_DEDISP_ROUNDS", "1")
+    else:
+        monkeypatch.delenv("CS_B200_DEDISP_ROUNDS", raising=False)
     g = GEOMS[geom]
     t = ours_tables(*g)
     raw = _rfi(fb_for(g, nblocks=nblocks, seed=3), t.spectra_per_subint,

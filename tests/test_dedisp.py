@@ -160,9 +160,16 @@ def test_gpu_device_entry_point_matches_host(gpu_ready):
 
 @needs_ref
 @pytest.mark.gpu
-def test_gpu_offsets_wider_than_shared_memory(gpu_ready):
-    """No DM group fits in shared memory: the direct kernel takes over, with
-    the same bits."""
+@pytest.mark.parametrize("direct", [False, True])
+def test_gpu_offsets_wider_than_shared_memory(gpu_ready, monkeypatch, direct):
+    """Offsets of ~70,000 samples: the staged kernel runs groups of one DM;
+    the direct kernel (the plan's choice when not even one DM's windows fit
+    in shared memory, forced here by CS_B200_DEDISP_DIRECT) gives the same
+    bits."""
+    if direct:
+        monkeypatch.setenv("CS_B200_DEDISP_DIRECT", "1")
+    else:
+        monkeypatch.delenv("CS_B200_DEDISP_DIRECT", raising=False)
     t = ours_tables(*WIDE)
     nb = 3 * t.blocks_per_read + 2
     raw = fb_for(WIDE, nblocks=nb, seed=3)
