@@ -24,37 +24,42 @@
  * the output holds min(numout, (floor((nb-1)/bpr) - 1) * W) points and every
  * one of them follows the formula above.
  *
- * Kernels (HBM layout: raw [nspec][nchan] u8 as read; S [nsub][sstride] u16;
- * out [ndm][out_stride] f32):
+ * Kernels (HBM layout: raw [nspec][nchan] u8 as read; S [nsub][sstride]
+ * 32-bit words, word w holding samples w (low half) and w + DM_P (high
+ * half); out [ndm][out_stride] f32):
  *   dd_subband_u8  one CTA per (slab of subbands, 256-sample tile): the
  *                  tile's raw rows plus the delay halo are copied
  *                  asynchronously into shared memory with padded rows (an
  *                  odd number of words: lanes over consecutive samples hit
  *                  consecutive banks), then each warp sums the channels of
- *                  one subband for 32 samples.  HBM-bound: 1 B read per
- *                  channel-sample, 2 B written per subband-sample.
- *   dd_dms_u16     one CTA per (group of up to 32 DMs, 256-sample tile): the
- *                  S windows the group needs (tile + the group's offset
- *                  spread) are staged in shared memory once, with a copy
- *                  shifted by one sample for odd offsets, and serve all the
- *                  group's DMs.  Each thread sums the subbands for 4 sample
- *                  pairs of 4 DMs with packed 16-bit adds (two samples per
- *                  32-bit add, widened before they can carry); lanes read
- *                  consecutive words.  Shared-memory-bound: 2 B of shared
- *                  reads per subband term.
+ *                  one subband for 32 samples and writes each sum into the
+ *                  two words that hold it.
+ *   dd_dms_u16     persistent, warp-specialised: a copy warp bulk-copies
+ *                  each work item's S windows (tile + the DM group's offset
+ *                  spread) and code block into a ring of shared stages; 16
+ *                  summing warps add one word per (DM, subband, column),
+ *                  i.e. two samples per 32-bit add (widened before the
+ *                  16-bit halves can carry).  Shared-memory-bound: 2 B of
+ *                  shared reads per subband term.
  *   dd_dms_u16_direct  the same sums straight from L1/L2, for geometries
  *                  whose windows do not fit in shared memory.
  *
  * A run with prepsubband's -clip that replaces spectra (cs_clip_levels) has
  * non-integer channel levels in it, so its sums need FP32 in the reference's
- * order; S is float there:
+ * order; S is float there (one sample per element):
  *   dd_subband_clip  dd_subband_u8's staging plus one clip flag per row;
  *                  channels added in ascending frequency from 0.0f, a
  *                  flagged spectrum contributing its block's level.
- *   dd_dms_f32     one CTA per (1024 samples, 16 DMs); per round of four
- *                  subbands the union windows are copied into shared memory
- *                  with cp.async a round ahead of the sums; subbands added in
- *                  ascending order from -0.0f.
+ *   dd_dms_f32_ws  dd_dms_u16's pipeline over float windows; each summing
+ *                  thread adds the subbands in ascending order from -0.0f
+ *                  for 2 DMs x 8 samples.
+ *   dd_dms_f32     the fallback for geometries whose stages do not fit
+ *                  twice: one CTA per (1024 samples, 16 DMs), per round of
+ *                  four subbands the union windows copied with cp.async a
+ *                  round ahead of the sums.
+ *
+ * Every wait in the pipelined kernels is bounded; one that gives up sets the
+ * plan's error flag (cs_dedisp_run and cs_dedisp_last_times report it).
  */
 #include <cuda_runtime.h>
 

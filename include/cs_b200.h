@@ -279,11 +279,13 @@ int cs_dedisp_run_device_clipped(CsDedisp *d, const uint8_t *d_raw, long long ns
                                  float *d_out, long long out_stride, void *stream,
                                  long long *nout_written);
 
-/* Host buffers; copies in and out and waits. */
+/* Host buffers; copies in and out and waits.  -1 also when a bounded wait
+ * inside the DM stage gave up (the output is then not valid). */
 int cs_dedisp_run(CsDedisp *d, const uint8_t *h_raw, long long nspec, long long numout,
                   float *h_out, long long out_stride, long long *nout_written);
 
-/* CUDA-event times of the last run's subband and DM kernels (ms). */
+/* CUDA-event times of the last run's subband and DM kernels (ms); waits for
+ * the run and returns -1 when one of its DM-stage waits gave up. */
 int cs_dedisp_last_times(CsDedisp *d, float *subband_ms, float *dm_ms);
 
 void cs_dedisp_free(CsDedisp *d);
