@@ -56,7 +56,7 @@ SIMT_OPS_PER_TRIAL = 6000.0       # interp 1920 FMA + 360 rotate + boxcar/fold ~
 
 
 KERNEL_NAMES = {0: "cs_search_kernel", 1: "search_ws_cfg60", 2: "search_f64",
-                3: "search_tma_cfg60"}
+                3: "search_tma_cfg60", 4: "interp_tc + search_pre_cfg60"}
 
 
 def load_peaks():

@@ -623,6 +623,7 @@ cs_search_kernel(const SearchArgs args)
 }
 
 #include "cs_search_ws.cuh"
+#include "cs_interp_tc.cuh"
 #include "cs_search_tma.cuh"
 #include "cs_search_f64.cuh"
 #include "cs_collapse.h"
@@ -694,6 +695,16 @@ struct GpuSession {
     float2 *d_tc[2];       /* zero-padded spectrum copies (second shifted a bin) */
     size_t c_wtab, c_cchunk, c_tc;
     wsk::TArgs tx;
+    /* interpolation as tensor-core GEMMs (tci::interp_tc), then search_pre */
+    int use_tci;
+    tci::Band *d_tci_bands;
+    uint4 *d_tci_bimg;
+    int *d_tci_hbase;
+    float2 *d_X;
+    size_t c_tci_bands, c_tci_bimg, c_X;
+    int tci_nband;
+    float tci_inv_sb;
+    long long tci_xstride;
     /* FP64 search (p->precision == CS_PREC_F64) */
     int prec64;
     f64k::Extra fx;
@@ -776,6 +787,10 @@ static void session_release(GpuSession *S)
     cudaFree(S->d_maps);
     cudaFree(S->d_tc[0]);
     cudaFree(S->d_tc[1]);
+    cudaFree(S->d_tci_bands);
+    cudaFree(S->d_tci_bimg);
+    cudaFree(S->d_tci_hbase);
+    cudaFree(S->d_X);
     cudaFree(S->d_bcs);
     cudaFree(S->d_scales);
     cudaFree(S->d_recs64);
@@ -876,6 +891,113 @@ static int ws_config(const CsTables &t, long long total)
 
 static cudaError_t dev_reserve(void **p, size_t *cap, size_t need);
 static uint32_t magic_for(int d);
+static int ws_smem(int nh);
+
+/* Tables of the tensor-core interpolation (cs_interp_tc.cuh) for the
+ * nharms 60 configuration (pnum 1, q a multiple of tci::NB): per (harmonic,
+ * band) the window start R_h(i0) and width, and the band's weight matrix
+ * with the rows' gains folded in, scaled by a power of two and split into
+ * fp16 hi + lo images in the canonical K-major layout; per harmonic the base
+ * bin.  Opt-in with CS_B200_TC_INTERP=1.  Returns false (the session keeps
+ * the single-kernel path) when the geometry does not fit. */
+static bool tci_load(GpuSession *S, const CsTables &t, long long total)
+{
+    using namespace tci;
+    if (S->use_ws != 60 || !getenv("CS_B200_TC_INTERP")) return false;
+    if (t.pnum != 1 || t.q % NB != 0 || t.m != 16) return false;
+    const int q = t.q, nh = t.nh, m = t.m, nband = q / NB;
+    if (nh * nband > MAXBAND || nh > 64) return false;
+    std::vector<Band> bands((size_t)nh * nband);
+    std::vector<int> hbase(nh);
+    std::vector<double> vals;          /* per band NOUT x kpad, row-major, before the split */
+    std::vector<int> voff((size_t)nh * nband);
+    double vmax = 0.0;
+    for (int h = 1; h <= nh; h++) {
+        const CsHarm &hm = t.harm[h - 1];
+        const int P = hm.P, woff = hm.woff, cr = t.carry_res[h - 1];
+        if (P < 1 || hm.rfloor0 + 1 - m / 2 < -(1LL << 30) || hm.rfloor0 > (1LL << 30)) return false;
+        hbase[h - 1] = (int)(hm.rfloor0 + 1 - m / 2);
+        auto R = [&](int i) {
+            const long long ih = (long long)i * h;
+            return (int)(ih / q) + ((ih % q) >= cr ? 1 : 0);
+        };
+        for (int b = 0; b < nband; b++) {
+            const int i0 = b * NB, rel = R(i0);
+            const int wb = R(i0 + NB - 1) - rel + m;
+            const int kpad = (2 * wb + 15) / 16 * 16;
+            if (kpad > KMAX) return false;
+            Band &bd = bands[(size_t)(h - 1) * nband + b];
+            bd.rel = rel;
+            bd.kpad = kpad;
+            bd.i0 = i0;
+            voff[(size_t)(h - 1) * nband + b] = (int)vals.size();
+            vals.resize(vals.size() + (size_t)NOUT * kpad, 0.0);
+            double *B = vals.data() + voff[(size_t)(h - 1) * nband + b];
+            for (int i = i0; i < i0 + NB; i++) {
+                const int ph = i % P;
+                const double gr = t.A[2 * (woff + ph)], gi = t.A[2 * (woff + ph) + 1];
+                const int nre = 2 * (i - i0);
+                for (int k = 0; k < m; k++) {
+                    const double w = t.W[(size_t)(woff + ph) * m + k];
+                    const int kk = R(i) - rel + k;
+                    B[(size_t)nre * kpad + 2 * kk] = gr * w;
+                    B[(size_t)nre * kpad + 2 * kk + 1] = -gi * w;
+                    B[(size_t)(nre + 1) * kpad + 2 * kk] = gi * w;
+                    B[(size_t)(nre + 1) * kpad + 2 * kk + 1] = gr * w;
+                }
+            }
+        }
+    }
+    for (double v : vals) vmax = std::max(vmax, std::fabs(v));
+    if (!(vmax > 0.0) || !(vmax < 1e30)) return false;
+    int e;
+    std::frexp(vmax, &e);                   /* vmax in [2^(e-1), 2^e) */
+    const double sb = std::ldexp(1.0, 14 - e);
+    /* images: per band hi then lo, NOUT x kpad halves each */
+    std::vector<uint16_t> img;
+    for (int j = 0; j < nh * nband; j++) {
+        Band &bd = bands[j];
+        bd.boff = (int)(img.size() / 8);
+        const size_t n = (size_t)NOUT * bd.kpad;
+        const size_t base = img.size();
+        img.resize(base + 2 * n, 0);
+        const double *B = vals.data() + voff[j];
+        for (int r = 0; r < NOUT; r++)
+            for (int k = 0; k < bd.kpad; k++) {
+                const double v = B[(size_t)r * bd.kpad + k] * sb;
+                const __half hi = __float2half_rn((float)v);
+                const __half lo = __float2half_rn((float)(v - (double)__half2float(hi)));
+                const size_t o = b_offset(NOUT, r, k) / 2;
+                img[base + o] = __half_as_ushort(hi);
+                img[base + n + o] = __half_as_ushort(lo);
+            }
+    }
+    const long long xstride = (total + 1) / 2 * 2;
+    if (dev_reserve((void **)&S->d_tci_bands, &S->c_tci_bands, bands.size() * sizeof(Band)) != cudaSuccess ||
+        dev_reserve((void **)&S->d_tci_bimg, &S->c_tci_bimg, img.size() * sizeof(uint16_t)) != cudaSuccess ||
+        dev_reserve((void **)&S->d_X, &S->c_X, (size_t)nh * xstride * sizeof(float2)) != cudaSuccess)
+        return false;
+    if (!S->d_tci_hbase && cudaMalloc((void **)&S->d_tci_hbase, sizeof(int) * CS_MAX_NH) != cudaSuccess)
+        return false;
+    if (cudaMemcpyAsync(S->d_tci_bands, bands.data(), bands.size() * sizeof(Band),
+                        cudaMemcpyHostToDevice, S->st) != cudaSuccess ||
+        cudaMemcpyAsync(S->d_tci_bimg, img.data(), img.size() * sizeof(uint16_t),
+                        cudaMemcpyHostToDevice, S->st) != cudaSuccess ||
+        cudaMemcpyAsync(S->d_tci_hbase, hbase.data(), sizeof(int) * nh, cudaMemcpyHostToDevice,
+                        S->st) != cudaSuccess)
+        return false;
+    /* pageable sources: the copies have read them when the stream gets here */
+    if (cudaStreamSynchronize(S->st) != cudaSuccess) return false;
+    if (cudaFuncSetAttribute((const void *)interp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             SMEM_BYTES) != cudaSuccess ||
+        cudaFuncSetAttribute((const void *)wsk::search_pre<wsk::Cfg60>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, ws_smem(60)) != cudaSuccess)
+        return false;
+    S->tci_nband = nband;
+    S->tci_inv_sb = (float)(1.0 / sb);
+    S->tci_xstride = xstride;
+    return true;
+}
 
 /* The column-tile kernel takes the search_ws configurations when the trial
  * grid has period q = 2*nharms (hidr 0.5, pnum 1): column tiles of q trials,
@@ -1247,7 +1369,9 @@ static int session_load(GpuSession *S, const FFTFile *ft, const SearchParams *p,
         CK(cudaMemcpyAsync(S->d_Wt, wfix.data(), wfix.size() * sizeof(float), cudaMemcpyHostToDevice, S->st));
         CK(ws_prepare(S->use_ws));
     }
-    S->use_tma = tma_config(t, total, S->namps, S->use_ws);
+    S->use_tci = tci_load(S, t, total) ? 1 : 0;
+    (void)cudaGetLastError();
+    S->use_tma = S->use_tci ? 0 : tma_config(t, total, S->namps, S->use_ws);
     if (S->use_tma && (tma_smem(S->use_tma) > S->max_smem || !tma_load(S, t, total)))
         S->use_tma = 0;
     {
@@ -1488,6 +1612,36 @@ static cudaError_t enqueue_search(GpuSession *S, const float2 *d_amps, double th
         if (timed) cudaEventRecord(S->ev1, S->st);
         return cudaGetLastError();
     }
+    if (S->use_ws && S->use_tci) {
+        tci::Args ta;
+        memset(&ta, 0, sizeof(ta));
+        ta.amps = d_amps;
+        ta.namps = S->namps;
+        ta.amax = S->d_amax;
+        ta.bands = S->d_tci_bands;
+        ta.bimg = S->d_tci_bimg;
+        ta.hbase = S->d_tci_hbase;
+        ta.nh = S->tab.nh;
+        ta.nband = S->tci_nband;
+        ta.q = S->tab.q;
+        ta.total = S->total;
+        ta.ncol = (S->total + S->tab.q - 1) / S->tab.q;
+        ta.nunits = (ta.ncol + tci::ROWS - 1) / tci::ROWS * ta.nh;
+        ta.inv_sb = S->tci_inv_sb;
+        ta.X = S->d_X;
+        ta.xstride = S->tci_xstride;
+        ta.err = S->d_err;
+        wsk::Args w = ws_args(S, d_amps, threshold);
+        w.X = S->d_X;
+        w.xstride = S->tci_xstride;
+        const int grid1 = (int)std::min<long long>(ta.nunits, S->nsm);
+        const int grid = std::min(S->tab.ntiles, S->nsm);
+        if (timed) cudaEventRecord(S->ev0, S->st);
+        tci::interp_tc<<<grid1, tci::NTHREADS, tci::SMEM_BYTES, S->st>>>(ta);
+        wsk::search_pre<wsk::Cfg60><<<grid, 512, ws_smem(60), S->st>>>(w);
+        if (timed) cudaEventRecord(S->ev1, S->st);
+        return cudaGetLastError();
+    }
     if (S->use_ws) {
         const wsk::Args w = ws_args(S, d_amps, threshold);
         if (S->use_tma) {
@@ -1683,7 +1837,7 @@ CS_EXPORT int cs_b200_session_info(const GpuSession *S, CsB200Info *info)
     info->smem_bytes = S->prec64 ? S->f64_smem : S->use_tma ? tma_smem(S->use_tma)
                      : S->use_ws ? ws_smem(S->use_ws) : smem_bytes(S->tab);
     info->grid = S->use_tma ? std::min(S->tx.nitems, S->nsm) : std::min(S->tab.ntiles, S->nsm);
-    info->kernel = S->prec64 ? 2 : S->use_tma ? 3 : S->use_ws ? 1 : 0;
+    info->kernel = S->prec64 ? 2 : S->use_tci ? 4 : S->use_tma ? 3 : S->use_ws ? 1 : 0;
     info->total = S->total;
     info->rec_capacity = S->cap;
     return 0;

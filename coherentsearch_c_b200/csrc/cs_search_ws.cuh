@@ -97,6 +97,9 @@ struct Args {
     unsigned *count;
     unsigned cap;
     int *err;
+    /* precomputed interpolation (search_pre): X[(h - 1) * xstride + t] */
+    const float2 *X;
+    long long xstride;
 };
 
 template <class WS>
@@ -380,6 +383,28 @@ static __device__ __forceinline__ void state_at(const Args &a, const TrialState 
  * arithmetic) and store them, split into fp16 hi/lo, as K block hb of the
  * A operand in tensor memory.  (res, qint) enter at h = 4hb+1 and leave at
  * h = 4hb+5. */
+/* Store 4 harmonics of one trial, scaled and split into fp16 hi/lo, as K
+ * block hb of the A operand in tensor memory. */
+template <int AHALF>
+static __device__ __forceinline__ void store_block(const float *xr4, const float *xi4, float scale,
+                                                   int hb, uint32_t abuf)
+{
+    uint32_t hw[4], lw[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        const float2 sc = make_float2(xr4[u] * scale, xi4[u] * scale);
+        const __half2 hi = __float22half2_rn(sc);
+        const float2 back = __half22float2(hi);
+        const __half2 lo = __float22half2_rn(
+            make_float2(__fsub_rn(sc.x, back.x), __fsub_rn(sc.y, back.y)));
+        hw[u] = *reinterpret_cast<const uint32_t *>(&hi);
+        lw[u] = *reinterpret_cast<const uint32_t *>(&lo);
+    }
+    /* K block hb = columns 4hb..4hb+3 (two halves per column); lo K/2 columns on */
+    tmem_st4(abuf + 4 * hb, hw[0], hw[1], hw[2], hw[3]);
+    tmem_st4(abuf + AHALF + 4 * hb, lw[0], lw[1], lw[2], lw[3]);
+}
+
 template <int AHALF>
 static __device__ __forceinline__ void interp_block(const Args &a, const Harm *hs,
                                                     const TrialState &ts, int hb,
@@ -387,7 +412,6 @@ static __device__ __forceinline__ void interp_block(const Args &a, const Harm *h
                                                     float scale, uint32_t abuf)
 {
     const uint32_t t = ts.t, R = ts.R, Q = ts.Q;
-    uint32_t hw[4], lw[4];
     const bool full = ts.valid && (((ts.filled >> (4 * hb)) & 0xFULL) == 0xFULL);
     float xr4[4], xi4[4];
     if (full) {
@@ -456,19 +480,7 @@ static __device__ __forceinline__ void interp_block(const Args &a, const Harm *h
             if (res >= (uint32_t)a.q) { res -= (uint32_t)a.q; qint += 1; }
         }
     }
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-        const float2 sc = make_float2(xr4[u] * scale, xi4[u] * scale);
-        const __half2 hi = __float22half2_rn(sc);
-        const float2 back = __half22float2(hi);
-        const __half2 lo = __float22half2_rn(
-            make_float2(__fsub_rn(sc.x, back.x), __fsub_rn(sc.y, back.y)));
-        hw[u] = *reinterpret_cast<const uint32_t *>(&hi);
-        lw[u] = *reinterpret_cast<const uint32_t *>(&lo);
-    }
-    /* K block hb = columns 4hb..4hb+3 (two halves per column); lo K/2 columns on */
-    tmem_st4(abuf + 4 * hb, hw[0], hw[1], hw[2], hw[3]);
-    tmem_st4(abuf + AHALF + 4 * hb, lw[0], lw[1], lw[2], lw[3]);
+    store_block<AHALF>(xr4, xi4, scale, hb, abuf);
 }
 
 /* Threshold one metric of slot S of this row (warp-aggregated compaction). */
@@ -506,6 +518,24 @@ struct Cfg60 {
             post<2>(a, ch, fold_metric<120, 3, W4>(trow, ch.invsw[2]) * inv, valid, ci, j, lane);
             post<3>(a, ch, fold_metric<120, 4, W4>(trow, ch.invsw[3]) * inv, valid, ci, j, lane);
             post<4>(a, ch, fold_metric<120, 5, W4>(trow, ch.invsw[4]) * inv, valid, ci, j, lane);
+        }
+    }
+    /* the same slots over four groups (search_pre): the base profile alone,
+     * then the folds paired by cost */
+    static __device__ __forceinline__ void epilogue4(int grp, uint32_t trow, const CsChunk &ch,
+                                                     const Args &a, bool valid, int ci, int j,
+                                                     int lane, float inv)
+    {
+        if (grp == 0) {
+            post<0>(a, ch, base_metric<120, W5>(trow, ch.invsw[0]) * inv, valid, ci, j, lane);
+        } else if (grp == 1) {
+            post<1>(a, ch, fold_metric<120, 2, W4>(trow, ch.invsw[1]) * inv, valid, ci, j, lane);
+            post<5>(a, ch, fold_metric<120, 6, W4>(trow, ch.invsw[5]) * inv, valid, ci, j, lane);
+        } else if (grp == 2) {
+            post<2>(a, ch, fold_metric<120, 3, W4>(trow, ch.invsw[2]) * inv, valid, ci, j, lane);
+            post<4>(a, ch, fold_metric<120, 5, W4>(trow, ch.invsw[4]) * inv, valid, ci, j, lane);
+        } else {
+            post<3>(a, ch, fold_metric<120, 4, W4>(trow, ch.invsw[3]) * inv, valid, ci, j, lane);
         }
     }
 };
@@ -951,6 +981,171 @@ __global__ void __launch_bounds__(nthreads<C>(), 1) search_ws(const __grid_const
 {
     const Multi none = {0, 0, 1};
     ws_body<C, false>(a, none);
+}
+
+/* The search with the interpolated values precomputed (X[h][t], by the
+ * tensor-core interpolation tci::interp_tc): all 16 warps in lockstep.
+ * Warp w owns trial rows 32 (w & 3) .. of a tile and group w >> 2.  Per
+ * tile it: load X of tile it + 2 (blocks g, g + 4, ... of the warp's rows),
+ * wait for the transform of tile it, run epilogue group g on it, store the
+ * loaded values as tile it + 2's A operand (its A buffer is free once the
+ * transform of tile it is done), barrier, then one thread issues the
+ * transform of tile it + 2.  Two transforms stay in flight behind the
+ * epilogue. */
+template <class C>
+static __device__ __forceinline__ void pre_body(const Args &a)
+{
+    constexpr int NH = C::NH, NPAD = C::NPAD, KPAD = C::KPAD, AHALF = KPAD / 2;
+    constexpr int NBLK = NH / 4;                       /* K blocks of 4 harmonics */
+    constexpr int JB = (NBLK + 3) / 4;                 /* blocks a warp */
+    constexpr int BIMG = NPAD * KPAD * 2;
+    constexpr int SM_B = 0, SM_BAR = 2 * BIMG, SM_TM = SM_BAR + 64;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int quarter = warp & 3, grp = warp >> 2;
+    const int r = quarter * 32 + lane;
+    const uint32_t tlane = (uint32_t)(quarter * 32) << 16;
+    const uint32_t bar_d = smem_u32(smem + SM_BAR);               /* 2 x 8 B */
+    uint32_t *tm_slot = reinterpret_cast<uint32_t *>(smem + SM_TM);
+    const int per_cta = (a.ntiles + gridDim.x - 1) / gridDim.x;
+    const int tile_begin = min(a.ntiles, (int)blockIdx.x * per_cta);
+    const int ntl = min(a.ntiles, tile_begin + per_cta) - tile_begin;
+
+    if (warp == 0) tmem_alloc(smem_u32(tm_slot), TMEM_COLS);
+    if (tid == 0) {
+        mbar_init(bar_d, 1);
+        mbar_init(bar_d + 8, 1);
+    }
+    {
+        uint4 *dst = reinterpret_cast<uint4 *>(smem + SM_B);
+        for (int i = tid; i < (2 * BIMG) / 16; i += blockDim.x) dst[i] = a.bimg[i];
+    }
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tm_slot;
+    const float scale = operand_scale(a.amax, a.gbound);
+    const float inv_scale = 1.0f / scale;
+    const uint32_t idesc = (1u << 4) | ((uint32_t)(NPAD >> 3) << 17) |
+                           ((uint32_t)(CS_TILE_M >> 4) << 24);
+    const uint32_t lbo_b = NPAD * 16;
+    const uint32_t b_hi = smem_u32(smem + SM_B), b_lo = b_hi + BIMG;
+
+    /* X of tile index i (0-based in the CTA's run) for the warp's blocks */
+    auto load_x = [&](int i, float2 (&xv)[JB][4]) {
+        const TrialState ts = trial_state(a, tile_begin + i, r);
+#pragma unroll
+        for (int jb = 0; jb < JB; jb++) {
+            const int hb = grp + 4 * jb;
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int h = 4 * hb + u + 1;
+                xv[jb][u] = (hb < NBLK && ts.valid && ((ts.filled >> (h - 1)) & 1ULL))
+                                ? __ldg(a.X + (long long)(h - 1) * a.xstride + ts.t)
+                                : make_float2(0.0f, 0.0f);
+            }
+        }
+    };
+    auto store_a = [&](int s, const float2 (&xv)[JB][4]) {
+        const uint32_t abuf = tmem + tlane + (uint32_t)(TM_A + KPAD * s);
+#pragma unroll
+        for (int jb = 0; jb < JB; jb++) {
+            const int hb = grp + 4 * jb;
+            if (hb >= NBLK) break;
+            const float xr4[4] = {xv[jb][0].x, xv[jb][1].x, xv[jb][2].x, xv[jb][3].x};
+            const float xi4[4] = {xv[jb][0].y, xv[jb][1].y, xv[jb][2].y, xv[jb][3].y};
+            store_block<AHALF>(xr4, xi4, scale, hb, abuf);
+        }
+    };
+    auto issue = [&](int s) {
+        const uint32_t a_hi = tmem + (uint32_t)(TM_A + KPAD * s), a_lo = a_hi + AHALF;
+        const uint32_t d = tmem + (uint32_t)(TM_D + D_STRIDE * s);
+        uint32_t acc = 0;
+#pragma unroll
+        for (int pass = 0; pass < 3; pass++) {
+            const uint32_t abase = (pass == 1) ? a_lo : a_hi;
+            const uint32_t bbase = (pass == 2) ? b_lo : b_hi;
+#pragma unroll
+            for (int k = 0; k < KPAD / 16; k++) {
+                mma_f16_ts(d, abase + (uint32_t)(8 * k),
+                           umma_desc(bbase + (uint32_t)k * 2 * lbo_b, lbo_b, 128), idesc, acc);
+                acc = 1;
+            }
+        }
+        mma_commit(bar_d + 8 * s);
+    };
+
+    /* the K padding columns (harmonics past nharms) of both A buffers stay zero */
+    if (grp == 0) {
+#pragma unroll
+        for (int b = 0; b < 2; b++) {
+            const uint32_t ab = tmem + tlane + (uint32_t)(TM_A + KPAD * b);
+#pragma unroll
+            for (int c = NH; c < AHALF; c += 4) {
+                tmem_st4(ab + c, 0, 0, 0, 0);
+                tmem_st4(ab + AHALF + c, 0, 0, 0, 0);
+            }
+        }
+    }
+    /* prologue: tiles 0 and 1 */
+    for (int i = 0; i < 2 && i < ntl; i++) {
+        float2 xv[JB][4];
+        load_x(i, xv);
+        store_a(i, xv);
+    }
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    int issued = 0;
+    if (tid == 0)
+        for (int i = 0; i < 2 && i < ntl; i++) issue(i);
+    issued = min(2, ntl);
+    bool ok = true;
+    for (int it = 0; it < ntl; it++) {
+        const int s = it & 1;
+        float2 xv[JB][4];
+        const bool next = it + 2 < ntl;
+        if (next) load_x(it + 2, xv);
+        const bool got = mbar_wait(bar_d + 8 * s, (it >> 1) & 1);
+        if (__syncthreads_or(!got)) {
+            if (tid == 0) atomicExch(a.err, 1);
+            ok = false;
+            break;
+        }
+        tc_fence_after();
+        {
+            const int tile = tile_begin + it;
+            const int ci = a.tiles[3 * tile], j0 = a.tiles[3 * tile + 1];
+            const int cnt = a.tiles[3 * tile + 2];
+            const CsChunk &ch = a.chunks[ci];
+            const uint32_t trow = tmem + (uint32_t)(TM_D + s * D_STRIDE) + tlane;
+            C::epilogue4(grp, trow, ch, a, r < cnt, ci, j0 + r, lane, inv_scale);
+        }
+        if (next) store_a(s, xv);
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (next && tid == 0) issue(s);
+        if (next) issued++;
+    }
+    /* never free tensor memory under a transform in flight */
+    if (!ok && tid == 0)
+        for (int k = issued > 2 ? issued - 2 : 0; k < issued; k++)
+            mbar_wait(bar_d + 8 * (k & 1), (k >> 1) & 1);
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, TMEM_COLS);
+    }
+}
+
+template <class C>
+__global__ void __launch_bounds__(512, 1) search_pre(const __grid_constant__ Args a)
+{
+    pre_body<C>(a);
 }
 
 /* The same kernel over the tiles of several spectra (search_ws_multi). */

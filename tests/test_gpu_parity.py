@@ -46,7 +46,7 @@ def match_candidates(a, b, thr, rtol):
     return only_a, only_b
 
 
-KERNEL_IDS = {"generic": 0, "ws": 1, "tma": 3}
+KERNEL_IDS = {"generic": 0, "ws": 1, "tma": 3, "tci": 4}
 
 
 def use_kernel(monkeypatch, kernel):
@@ -54,14 +54,17 @@ def use_kernel(monkeypatch, kernel):
     the ladder it covers), the register-staged search_ws, or the generic one."""
     monkeypatch.delenv("CS_B200_GENERIC_KERNEL", raising=False)
     monkeypatch.delenv("CS_B200_WS_KERNEL", raising=False)
+    monkeypatch.delenv("CS_B200_TC_INTERP", raising=False)
     monkeypatch.setenv("CS_B200_TMA_KERNEL", "1")
-    if kernel == "generic":
+    if kernel == "tci":
+        monkeypatch.setenv("CS_B200_TC_INTERP", "1")
+    elif kernel == "generic":
         monkeypatch.setenv("CS_B200_GENERIC_KERNEL", "1")
     elif kernel == "ws":
         monkeypatch.setenv("CS_B200_WS_KERNEL", "1")
 
 
-@pytest.mark.parametrize("nharms,kernel", [(60, "tma"), (32, "tma"), (16, "tma"), (60, "ws"),
+@pytest.mark.parametrize("nharms,kernel", [(60, "tci"), (60, "tma"), (32, "tma"), (16, "tma"), (60, "ws"),
                                            (32, "ws"), (16, "ws"), (60, "generic"),
                                            (32, "generic"), (16, "generic"), (7, "generic")])
 def test_all_trial_metrics_vs_oracle(gpu_ready, monkeypatch, nharms, kernel):
