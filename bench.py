@@ -967,7 +967,7 @@ def sweep_lines(files, slots, nh_list, steps, warmup, ref_gpu, device=0):
     from coherentsearch_c_b200 import synth
     from coherentsearch_c_b200.batch import Batch
     from coherentsearch_c_b200 import native as nt
-    from coherentsearch_c_b200.search import Options, Session, multi_search
+    from coherentsearch_c_b200.search import MultiGraph, Options, Session, multi_search
     from coherentsearch_c_b200.sweep import autotune, search_list, warm
     specs = synth.config_dm_sweep(n_files=files)
     dt = specs[0].dt
@@ -1048,6 +1048,22 @@ def sweep_lines(files, slots, nh_list, steps, warmup, ref_gpu, device=0):
                 e1.synchronize()
                 rts.append(e0.elapsed_time(e1))
                 rks.append(kms)
+            # the same launch recorded once as a CUDA graph and replayed
+            graph = MultiGraph(resident, ptrs)
+            try:
+                graph.search(stream=st)                            # warm
+                gts = []
+                for _ in range(max(1, min(steps, 2))):
+                    torch.cuda.synchronize()
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    gout, _ = graph.search(stream=st)
+                    e1.record(stream)
+                    e1.synchronize()
+                    gts.append(e0.elapsed_time(e1))
+            finally:
+                graph.close()
         finally:
             for ses in resident:
                 ses.close()
@@ -1071,6 +1087,10 @@ def sweep_lines(files, slots, nh_list, steps, warmup, ref_gpu, device=0):
                      "resident_one_launch_kernel_ms": statistics.mean(rks),
                      "resident_equal_candidates": bool(all(
                          _same_cands(x, y) for x, y in zip(rout, res["plain"][1]))),
+                     "resident_graph_ms": statistics.mean(gts),
+                     "resident_graph_trials_per_s": trials / (statistics.mean(gts) * 1e-3),
+                     "resident_graph_equal_candidates": bool(all(
+                         _same_cands(x, y) for x, y in zip(gout, res["plain"][1]))),
                      "equal_candidates": bool(equal), "differing_files": diff,
                      "candidates": int(sum(o.size for o in res["batched"][1])),
                      "plain_candidates": int(sum(o.size for o in res["plain"][1]))}

@@ -681,6 +681,10 @@ struct GpuSession {
     size_t h_recs_cap;
     float last_kernel_ms;
     int own_plans;
+    /* bumped whenever the tables or the record buffer may move (a reload, a
+     * record buffer grown): a captured launch that baked in their addresses
+     * checks it before each replay */
+    unsigned gen;
     /* warp-specialised kernel (default ladder at nharms = 60) */
     int use_ws;
     float4 *d_Wt;
@@ -847,6 +851,7 @@ static int grow_records64(GpuSession *S, unsigned cap)
 
 static int grow_records(GpuSession *S, unsigned cap)
 {
+    S->gen++;
     cudaFree(S->d_recs);
     S->d_recs = NULL;
     S->cap = 0;
@@ -1245,6 +1250,7 @@ static int session_load(GpuSession *S, const FFTFile *ft, const SearchParams *p,
     std::vector<uint16_t> bhi, blo;
     size_t img_halves = 0;
     int smem = 0;
+    S->gen++;
     S->p = p;
     S->Nprof = Nprof;
     S->total = total;
@@ -1982,6 +1988,25 @@ static cudaError_t multi_launch(int nh, int grid, cudaStream_t st, const wsk::Ar
     return cudaLaunchKernel(fn, dim3(grid), dim3(nthr), args, (size_t)ws_smem_multi(nh), st);
 }
 
+/* The sessions of one multi-spectrum launch: FP32, one device, one
+ * warp-specialised configuration (nharms and ladder). */
+static bool multi_compatible(GpuSession *const *ss, int n)
+{
+    const GpuSession *S0 = ss[0];
+    for (int i = 0; i < n; i++) {
+        const GpuSession *S = ss[i];
+        if (!S || !S0 || S->device != S0->device || S->prec64 || !S->use_ws ||
+            S->use_ws != S0->use_ws || S->tab.nslot != S0->tab.nslot ||
+            S->tab.npad != S0->tab.npad || S->tab.kpad != S0->tab.kpad ||
+            memcmp(S->tab.slot, S0->tab.slot, sizeof(CsSlot) * (size_t)S0->tab.nslot) != 0) {
+            fprintf(stderr, "Error: a multi-spectrum launch takes FP32 sessions of one "
+                            "warp-specialised configuration (same nharms and ladder)\n");
+            return false;
+        }
+    }
+    return true;
+}
+
 CS_EXPORT int cs_b200_multi_enqueue(GpuSession **ss, int n, const float *const *d_amps,
                                     double threshold, void *stream)
 {
@@ -2001,17 +2026,7 @@ CS_EXPORT int cs_b200_multi_enqueue(GpuSession **ss, int n, const float *const *
         return -1;
     }
     GpuSession *S0 = ss[0];
-    for (int i = 0; i < n; i++) {
-        const GpuSession *S = ss[i];
-        if (!S || S->device != S0->device || S->prec64 || !S->use_ws || S->use_ws != S0->use_ws ||
-            S->tab.nslot != S0->tab.nslot || S->tab.npad != S0->tab.npad ||
-            S->tab.kpad != S0->tab.kpad ||
-            memcmp(S->tab.slot, S0->tab.slot, sizeof(CsSlot) * (size_t)S0->tab.nslot) != 0) {
-            fprintf(stderr, "Error: a multi-spectrum launch takes FP32 sessions of one "
-                            "warp-specialised configuration (same nharms and ladder)\n");
-            return -1;
-        }
-    }
+    if (!multi_compatible(ss, n)) return -1;
     const int dev = S0->device;
     if (dev < 0 || dev >= 64) return -1;
     MCK(select_device(dev));
@@ -2065,6 +2080,186 @@ CS_EXPORT int cs_b200_multi_enqueue(GpuSession **ss, int n, const float *const *
         if (ss[i]->st != st) MCK(cudaStreamWaitEvent(ss[i]->st, M.done, 0));
     return 0;
 #undef MCK
+}
+
+/* ------------------------------------------------------------------ */
+/* A multi-spectrum search captured as a CUDA graph                    */
+/* ------------------------------------------------------------------ */
+/* The per-spectrum clears and maxima, the copy of the argument table and
+ * tile offsets into constant memory, and the persistent launch over all the
+ * spectra's tiles, recorded once by stream capture and replayed as one graph
+ * launch.  The graph bakes in each session's buffer addresses, so it records
+ * each session's generation and refuses to replay after a reload or a grown
+ * record buffer.  The table copies read pinned host memory that the graph
+ * object owns. */
+struct CsMultiGraph {
+    int device = -1;
+    std::vector<GpuSession *> ss;
+    std::vector<unsigned> gen;
+    wsk::Args *h_files = nullptr;   /* pinned: constant-table copy source */
+    int *h_off = nullptr;           /* pinned */
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t cap = nullptr;     /* capture stream */
+};
+
+static void multi_graph_release(CsMultiGraph *G)
+{
+    if (!G) return;
+    if (G->exec) cudaGraphExecDestroy(G->exec);
+    if (G->cap) cudaStreamDestroy(G->cap);
+    if (G->h_files) cudaFreeHost(G->h_files);
+    if (G->h_off) cudaFreeHost(G->h_off);
+    delete G;
+}
+
+/* The captured body: one stream, no events, no host synchronisation. */
+static cudaError_t multi_graph_body(CsMultiGraph *G, int nh, int grid, int nsm, int ntiles,
+                                    const float *const *d_amps)
+{
+    cudaError_t e;
+    const cudaStream_t st = G->cap;
+    const int n = (int)G->ss.size();
+    for (int i = 0; i < n; i++) {
+        GpuSession *S = G->ss[(size_t)i];
+        const float2 *amps = d_amps && d_amps[i] ? (const float2 *)d_amps[i] : S->d_amps;
+        if ((e = cudaMemsetAsync(S->d_amax, 0, 2 * sizeof(unsigned), st)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(S->d_count, 0, sizeof(unsigned), st)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(S->d_err, 0, sizeof(int), st)) != cudaSuccess) return e;
+        if (S->namps > 0) {
+            const int gr = (int)std::min<long long>((S->namps + 255) / 256, (long long)nsm * 8);
+            cs_amax_kernel<<<gr, 256, 0, st>>>(amps, S->namps, S->d_amax);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+    }
+    if (ntiles <= 0) return cudaSuccess;
+    if ((e = cudaMemcpyToSymbolAsync(wsk::c_multi_files, G->h_files, (size_t)n * sizeof(wsk::Args),
+                                     0, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return e;
+    if ((e = cudaMemcpyToSymbolAsync(wsk::c_multi_off, G->h_off, (size_t)(n + 1) * sizeof(int), 0,
+                                     cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return e;
+    wsk::Multi mu;
+    mu.nfiles = n;
+    mu.ntiles = ntiles;
+    mu.block = 64;
+    if (const char *v = getenv("CS_B200_MULTI_BLOCK")) mu.block = std::max(1, atoi(v));
+    return multi_launch(nh, grid, st, G->h_files[0], mu);
+}
+
+CS_EXPORT CsMultiGraph *cs_b200_multi_graph_create(GpuSession **ss, int n,
+                                                   const float *const *d_amps, double threshold)
+{
+    if (!ss || n < 1) return nullptr;
+    if (n > wsk::MULTI_MAX) {
+        fprintf(stderr, "Error: a multi-spectrum graph takes at most %d spectra (got %d)\n",
+                wsk::MULTI_MAX, n);
+        return nullptr;
+    }
+    if (!multi_compatible(ss, n)) return nullptr;
+    GpuSession *S0 = ss[0];
+    const int dev = S0->device;
+    if (dev < 0 || dev >= 64 || select_device(dev) != cudaSuccess) return nullptr;
+    CsMultiGraph *G = new CsMultiGraph();
+    G->device = dev;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaSuccess;
+    const char *what = "";
+#define GCK(call)                                                                 \
+    do {                                                                          \
+        if ((e = (call)) != cudaSuccess) { what = #call; goto fail; }             \
+    } while (0)
+    {
+        G->ss.assign(ss, ss + n);
+        G->gen.resize((size_t)n);
+        GCK(cudaMallocHost((void **)&G->h_files, (size_t)n * sizeof(wsk::Args)));
+        GCK(cudaMallocHost((void **)&G->h_off, (size_t)(n + 1) * sizeof(int)));
+        G->h_off[0] = 0;
+        for (int i = 0; i < n; i++) {
+            GpuSession *S = ss[i];
+            const float2 *amps = d_amps && d_amps[i] ? (const float2 *)d_amps[i] : S->d_amps;
+            G->gen[(size_t)i] = S->gen;
+            G->h_files[i] = ws_args(S, amps, threshold);
+            G->h_off[i + 1] = G->h_off[i] + S->tab.ntiles;
+        }
+        const int ntiles = G->h_off[n];
+        const int grid = std::min(std::max(ntiles, 1), S0->nsm);
+        /* attributes are set outside the capture */
+        GCK(ws_prepare_multi(S0->use_ws));
+        GCK(cudaStreamCreateWithFlags(&G->cap, cudaStreamNonBlocking));
+        /* thread-local capture: other threads' calls (batch slots) stay legal */
+        GCK(cudaStreamBeginCapture(G->cap, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t eb = multi_graph_body(G, S0->use_ws, grid, S0->nsm, ntiles, d_amps);
+        const cudaError_t ee = cudaStreamEndCapture(G->cap, &graph);
+        GCK(eb);
+        GCK(ee);
+        GCK(cudaGraphInstantiate(&G->exec, graph, 0ULL));
+        cudaGraphDestroy(graph);
+        graph = nullptr;
+    }
+#undef GCK
+    return G;
+fail:
+    fprintf(stderr, "Error: multi-spectrum graph: %s failed: %s\n", what, cudaGetErrorString(e));
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    multi_graph_release(G);
+    return nullptr;
+}
+
+CS_EXPORT int cs_b200_multi_graph_launch(CsMultiGraph *G, void *stream)
+{
+#define GLCK(call)                                                                \
+    do {                                                                          \
+        const cudaError_t e_ = (call);                                            \
+        if (e_ != cudaSuccess) {                                                  \
+            fprintf(stderr, "Error: multi-spectrum graph launch: %s failed: %s\n", \
+                    #call, cudaGetErrorString(e_));                               \
+            return -1;                                                            \
+        }                                                                         \
+    } while (0)
+    if (!G || !G->exec) return -1;
+    const int n = (int)G->ss.size();
+    for (int i = 0; i < n; i++)
+        if (G->ss[(size_t)i]->gen != G->gen[(size_t)i]) {
+            fprintf(stderr, "Error: multi-spectrum graph: session %d was reloaded or its record "
+                            "buffer grew after the capture; create the graph again\n", i);
+            return -2;
+        }
+    GLCK(select_device(G->device));
+    GpuSession *S0 = G->ss[0];
+    cudaStream_t st = stream ? (cudaStream_t)stream : S0->st;
+    std::lock_guard<std::mutex> g(g_multi_mu);
+    MultiTables &M = g_multi[G->device];
+    if (!M.done) GLCK(cudaEventCreateWithFlags(&M.done, cudaEventDisableTiming));
+    for (int i = 0; i < n; i++) {
+        GpuSession *S = G->ss[(size_t)i];
+        if (st != S->st) {
+            GLCK(cudaEventRecord(S->ev_in, S->st));
+            GLCK(cudaStreamWaitEvent(st, S->ev_in, 0));
+        }
+    }
+    /* the previous launch on this device may still read the constant tables */
+    GLCK(cudaStreamWaitEvent(st, M.done, 0));
+    GLCK(cudaEventRecord(S0->ev0, st));
+    GLCK(cudaGraphLaunch(G->exec, st));
+    GLCK(cudaEventRecord(S0->ev1, st));
+    GLCK(cudaEventRecord(M.done, st));
+    for (int i = 0; i < n; i++)
+        if (G->ss[(size_t)i]->st != st) GLCK(cudaStreamWaitEvent(G->ss[(size_t)i]->st, M.done, 0));
+    return 0;
+#undef GLCK
+}
+
+CS_EXPORT void cs_b200_multi_graph_free(CsMultiGraph *G)
+{
+    if (!G) return;
+    if (select_device(G->device) == cudaSuccess) {
+        /* a replay in flight still reads the pinned tables */
+        for (GpuSession *S : G->ss) cudaStreamSynchronize(S->st);
+        std::lock_guard<std::mutex> g(g_multi_mu);
+        if (g_multi[G->device].done) cudaEventSynchronize(g_multi[G->device].done);
+    }
+    multi_graph_release(G);
 }
 
 #ifdef WSK_TMA_PROF

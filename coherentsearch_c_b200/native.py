@@ -146,6 +146,13 @@ def declare_gpu_api(lib: C.CDLL) -> C.CDLL:
     lib.cs_b200_multi_enqueue.argtypes = [C.POINTER(C.c_void_p), C.c_int,
                                           C.POINTER(C.c_void_p), C.c_double, C.c_void_p]
     lib.cs_b200_multi_enqueue.restype = C.c_int
+    lib.cs_b200_multi_graph_create.argtypes = [C.POINTER(C.c_void_p), C.c_int,
+                                               C.POINTER(C.c_void_p), C.c_double]
+    lib.cs_b200_multi_graph_create.restype = C.c_void_p
+    lib.cs_b200_multi_graph_launch.argtypes = [C.c_void_p, C.c_void_p]
+    lib.cs_b200_multi_graph_launch.restype = C.c_int
+    lib.cs_b200_multi_graph_free.argtypes = [C.c_void_p]
+    lib.cs_b200_multi_graph_free.restype = None
     lib.cs_b200_session_enqueue_device.argtypes = [C.c_void_p, C.c_void_p, C.c_double,
                                                    C.c_void_p]
     lib.cs_b200_session_enqueue_device.restype = C.c_int

@@ -337,3 +337,54 @@ def multi_search(sessions, d_amps=None, threshold: float | None = None, stream=N
         return [], 0.0
     multi_enqueue(sessions, d_amps, threshold, stream)
     return multi_collect(sessions, d_amps, threshold)
+
+
+class MultiGraph:
+    """A multi-spectrum search recorded once as a CUDA graph
+    (cs_b200_multi_graph_create) and replayed with launch(); collect() gives
+    each session's raw candidates, as multi_collect does after
+    multi_enqueue.  The graph holds the sessions' buffer addresses: close it
+    before the sessions, and build a new one after a session is reloaded or
+    grows its record buffer (launch raises StaleGraph then)."""
+
+    class StaleGraph(RuntimeError):
+        pass
+
+    def __init__(self, sessions, d_amps=None, threshold: float | None = None):
+        self.gpu = nt.gpu_lib()
+        self.sessions = list(sessions)
+        self.d_amps = d_amps
+        self.threshold = self.sessions[0].opts.threshold if threshold is None else threshold
+        n = len(self.sessions)
+        arr = (C.c_void_p * n)(*[s.sess for s in self.sessions])
+        amps = None
+        if d_amps is not None:
+            amps = (C.c_void_p * n)(*[int(p) if p else None for p in d_amps])
+        self.graph = self.gpu.cs_b200_multi_graph_create(arr, n, amps, self.threshold)
+        if not self.graph:
+            raise RuntimeError("cs_b200_multi_graph_create failed")
+
+    def launch(self, stream=None) -> None:
+        rc = self.gpu.cs_b200_multi_graph_launch(self.graph, stream)
+        if rc == -2:
+            raise MultiGraph.StaleGraph("a session changed since the capture")
+        if rc != 0:
+            raise RuntimeError("cs_b200_multi_graph_launch failed")
+
+    def collect(self):
+        return multi_collect(self.sessions, self.d_amps, self.threshold)
+
+    def search(self, stream=None):
+        self.launch(stream)
+        return self.collect()
+
+    def close(self) -> None:
+        if getattr(self, "graph", None):
+            self.gpu.cs_b200_multi_graph_free(self.graph)
+            self.graph = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

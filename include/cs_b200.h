@@ -51,6 +51,28 @@ int cs_b200_session_info(const GpuSession *s, CsB200Info *info);
 int cs_b200_multi_enqueue(GpuSession **ss, int n, const float *const *d_amps,
                           double threshold, void *stream);
 
+/* The same multi-spectrum search recorded once as a CUDA graph and replayed
+ * (no counterpart in the reference; its list driver makes one search call
+ * per file, src/cli.c:976-1099, src/search.c:1292-1341).  create captures,
+ * on a private stream, what cs_b200_multi_enqueue queues: each spectrum's
+ * counter clears and maximum, the argument-table copy into constant memory
+ * (from pinned memory the graph owns) and the persistent launch.  launch
+ * replays it on `stream` (NULL: the first session's stream) after the work
+ * queued on every session's stream, and every session's stream then waits
+ * for it, so cs_b200_session_collect returns each session's candidates --
+ * equal to those of cs_b200_multi_enqueue on the same spectra.  The graph
+ * holds the sessions' buffer and spectrum addresses: launch returns -2 when
+ * a session was reloaded or grew its record buffer since the capture (an
+ * overflow that collect reported), and the graph must be freed before any of
+ * its sessions.  Replays on one device are serialised like
+ * cs_b200_multi_enqueue.  create returns NULL with a message on error;
+ * launch returns 0, -2, or -1 with a message. */
+typedef struct CsMultiGraph CsMultiGraph;
+CsMultiGraph *cs_b200_multi_graph_create(GpuSession **ss, int n, const float *const *d_amps,
+                                         double threshold);
+int cs_b200_multi_graph_launch(CsMultiGraph *g, void *stream);
+void cs_b200_multi_graph_free(CsMultiGraph *g);
+
 /* Device address of the session's spectrum buffer (namps float2). */
 float *cs_b200_session_device_amps(GpuSession *s);
 

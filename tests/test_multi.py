@@ -12,7 +12,7 @@ import pytest
 
 import refbind as rb
 from coherentsearch_c_b200 import synth
-from coherentsearch_c_b200.search import Options, Session, multi_search
+from coherentsearch_c_b200.search import MultiGraph, Options, Session, multi_search
 
 pytestmark = pytest.mark.gpu
 
@@ -63,3 +63,46 @@ def test_multi_launch_refuses_mixed_configurations(gpu_ready):
     finally:
         s60.close()
         s32.close()
+
+
+def test_multi_graph_replays_equal_multi_launch(gpu_ready, monkeypatch):
+    """The launch recorded as a CUDA graph gives, replay after replay, the
+    candidates of cs_b200_multi_enqueue on the same spectra; a session whose
+    record buffer grew makes the graph refuse to replay."""
+    monkeypatch.delenv("CS_B200_GENERIC_KERNEL", raising=False)
+    monkeypatch.delenv("CS_B200_TMA_KERNEL", raising=False)
+    data = _spectra([16, 18, 17, 16, 19], seed0=940)
+    opts = Options(nharms=60, blocksize=2048, threshold=6.0)
+    sessions = []
+    for N, amps in data:
+        ses = Session(N, 64e-6, opts)
+        assert ses.info().kernel == 1
+        ses.run_raw(amps)
+        sessions.append(ses)
+    try:
+        ref, _ = multi_search(sessions)
+        g = MultiGraph(sessions)
+        try:
+            for _ in range(3):
+                got, _ = g.search()
+                for a, b in zip(got, ref):
+                    assert a.size == b.size and a.size > 0
+                    np.testing.assert_array_equal(a["r"], b["r"])
+                    np.testing.assert_array_equal(a["nharm"], b["nharm"])
+                    np.testing.assert_array_equal(a["metric"], b["metric"])
+        finally:
+            g.close()
+        # every valid (trial, slot) is recorded at this threshold: the 2^19
+        # spectrum's record buffer overflows and grows
+        g = MultiGraph(sessions, threshold=-1e30)
+        try:
+            g.launch()
+            rcs = [s.collect(-1e30)[2] for s in sessions]
+            assert rcs[4] == 1
+            with pytest.raises(MultiGraph.StaleGraph):
+                g.launch()
+        finally:
+            g.close()
+    finally:
+        for s in sessions:
+            s.close()
