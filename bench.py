@@ -172,6 +172,77 @@ def cpu_reference_rate(amps, N, seconds=10.0, max_reps=50):
     return total * reps / dt, cores, sample
 
 
+def _ref_process(path, N, dt, barrier, results):
+    """One process of the reference's process-per-core deployment: one
+    OpenMP thread, one search of the spectrum at `path` after the barrier."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import refbind as rb
+    from coherentsearch_c_b200.search import Options
+    amps = np.ascontiguousarray(np.load(path))
+    opts = Options(blocksize=BLOCKSIZE_CPU, threshold=8.0)
+    rb.ref_lib()
+    rb.pin_ref_threads(1)
+    barrier.wait()
+    t0 = time.perf_counter()
+    rb.ref_search(amps, N, dt, opts)
+    results.put(time.perf_counter() - t0)
+
+
+def cpu_reference_forms(amps, N, nproc=None):
+    """The reference CPU path in its other two forms: one thread, and one
+    single-threaded process per host core each searching the whole spectrum
+    (the process-per-core deployment its README describes).  Processes are
+    spawned, never forked, so a CUDA context in this process is not copied.
+    Returns {"one_thread": ..., "processes": ...} in trials/s."""
+    import multiprocessing as mp
+    import tempfile
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import refbind as rb
+    from coherentsearch_c_b200.search import Options
+    dt = WORKLOAD["dt"]
+    opts = Options(blocksize=BLOCKSIZE_CPU, threshold=8.0)
+    _, _, total = opts.geometry(N, dt)
+    rb.ref_lib()
+    rb.pin_ref_threads(1)
+    t0 = time.perf_counter()
+    rb.ref_search(amps, N, dt, opts)
+    one = total / (time.perf_counter() - t0)
+    rb.pin_ref_threads(os.cpu_count() or 1)
+    nproc = nproc or (os.cpu_count() or 1)
+    ctx = mp.get_context("spawn")
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "amps.npy")
+        np.save(path, np.ascontiguousarray(amps))
+        barrier = ctx.Barrier(nproc)
+        results = ctx.Queue()
+        procs = [ctx.Process(target=_ref_process, args=(path, N, dt, barrier, results))
+                 for _ in range(nproc)]
+        for p in procs:
+            p.start()
+        times = []
+        try:
+            deadline = time.perf_counter() + 600.0
+            while len(times) < nproc:
+                try:
+                    times.append(results.get(timeout=1.0))
+                except Exception:   # noqa: BLE001  (queue.Empty)
+                    if (time.perf_counter() > deadline or
+                            not any(p.is_alive() for p in procs)):
+                        raise RuntimeError(f"{nproc - len(times)} reference processes "
+                                           "ended without a result")
+        finally:
+            for p in procs:
+                p.join(timeout=10)
+                if p.is_alive():
+                    p.terminate()
+    return {"one_thread": {"value": one, "cores": 1,
+                           "sample": f"one full search ({total} trials), one OpenMP thread"},
+            "processes": {"value": nproc * total / max(times), "cores": nproc,
+                          "sample": f"{nproc} single-threaded processes, each one full search "
+                                    f"({total} trials), started together; slowest "
+                                    f"{max(times):.2f} s"}}
+
+
 def precision_study(ses, amps, N, dt, opts, device):
     """The FP32 search (tensor-core fp16-split DFT) against this repository's
     FP64 search (--precision f64: FP64 DFT, folds and boxcar), the FP64
@@ -445,6 +516,10 @@ def run_b200(args):
             rate, cores, sample = cpu_reference_rate(amps, N, seconds=args.cpu_seconds)
             line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores,
                                     "kind": "reference", "sample": sample}
+            try:
+                line["cpu_baseline"]["forms"] = cpu_reference_forms(amps, N)
+            except Exception as exc:   # noqa: BLE001
+                line["cpu_baseline"]["forms"] = {"unavailable": str(exc)}
         except Exception as exc:   # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0,
                                     "kind": "reference", "sample": f"unavailable: {exc}"}
@@ -997,10 +1072,14 @@ def sweep_lines(files, slots, nh_list, steps, warmup, ref_gpu, device=0):
                 ses.close()
             return out
 
+        # a long-lived engine, as a serving process keeps one: created and its
+        # slots loaded for the longest file before the timed region
+        engine = Batch(nslots=slots)
+        engine.warm(max(sp.N for sp in specs), dt, opts)
+
         def batched():
-            with Batch(nslots=slots) as b:
-                ids = [b.submit(a, sp.N, dt, opts) for sp, a in zip(specs, spectra)]
-                return [b.wait(i)[0] for i in ids]
+            ids = [engine.submit(a, sp.N, dt, opts) for sp, a in zip(specs, spectra)]
+            return [engine.wait(i)[0] for i in ids]
 
         st = torch.cuda.current_stream().cuda_stream
         warm(max(sp.N for sp in specs), dt, opts, 64, device)   # two groups of up to 32
@@ -1012,9 +1091,8 @@ def sweep_lines(files, slots, nh_list, steps, warmup, ref_gpu, device=0):
             return search_list(listed, dt, opts, group, device, upload, st)
 
         for _ in range(warmup):           # warm: modules, allocator, page cache
-            with Batch(nslots=slots) as b:
-                for i in [b.submit(a, sp.N, dt, opts) for sp, a in zip(specs[:4], spectra[:4])]:
-                    b.wait(i)
+            for i in [engine.submit(a, sp.N, dt, opts) for sp, a in zip(specs[:4], spectra[:4])]:
+                engine.wait(i)
         stream = torch.cuda.current_stream()
         res = {}
         for name, fn in (("plain", plain), ("batched", batched), ("grouped", grouped)):
@@ -1029,6 +1107,7 @@ def sweep_lines(files, slots, nh_list, steps, warmup, ref_gpu, device=0):
                 e1.synchronize()
                 ts.append(e0.elapsed_time(e1))
             res[name] = (statistics.mean(ts), out)
+        engine.close()
         # every spectrum resident on the device, searched by ONE persistent
         # launch over all their tiles (the kernel-side bound of the grouped form)
         for i in range(len(specs)):
