@@ -1260,6 +1260,23 @@ def serve_capacity(reqs, maxlen, slots, budget_gb):
                                          zip(served["results"], plain["results"])))}
 
 
+def serve_load_curve(reqs, maxlen, slots, budget_gb, rates=(200, 400, 600, 800)):
+    """Latency against offered load: the same requests as open-loop Poisson
+    streams at each rate, through one engine loaded for the largest request.
+    Past the capacity the queue grows for the whole stream and p99 with it."""
+    from coherentsearch_c_b200.search import Options
+    from coherentsearch_c_b200.serve import SearchServer, poisson_arrivals, run_stream
+    curve = []
+    with SearchServer(nslots=slots, mem_budget=budget_gb << 30) as srv:
+        srv.warm(maxlen, 64e-6, Options(nharms=60, blocksize=65536, threshold=8.0))
+        for rate in rates:
+            res = run_stream(srv, reqs, poisson_arrivals(len(reqs), rate=rate, seed=3))
+            curve.append({"offered_per_s": rate, "p50_ms": res["p50_ms"],
+                          "p99_ms": res["p99_ms"], "trials_per_s": res["trials_per_s"],
+                          "requests_per_s": len(reqs) / res["wall_s"]})
+    return curve
+
+
 def serve_summary(nreq, rate, npool, slots, budget_gb, ref_gpu):
     """Config 5 in short: an open-loop Poisson stream at `rate` (served and
     plain, p50/p99 from arrival to result), then the closed-loop capacity of
@@ -1289,7 +1306,8 @@ def serve_summary(nreq, rate, npool, slots, budget_gb, ref_gpu):
                          "equal_candidates": bool(all(_same_cands(x, y) for x, y in
                                                       zip(served["results"],
                                                           plain["results"])))},
-           "closed_loop": serve_capacity(reqs, maxlen, slots, budget_gb)}
+           "closed_loop": serve_capacity(reqs, maxlen, slots, budget_gb),
+           "load_curve": serve_load_curve(reqs, maxlen, slots, budget_gb)}
     if ref_gpu:
         p0 = serve_reference_gpu(reqs, served["results"], served["trials_per_s"], limit=30)
         out["plain_reference_gpu"] = p0
@@ -1358,6 +1376,7 @@ def run_serve(args):
         "gpu_launches": 2 * len(reqs),
         "clocks": clk.summary(),
     }
+    line["load_curve"] = serve_load_curve(reqs, maxlen, args.slots, args.mem_budget_gb)
     if not args.no_ref_gpu:
         line["plain_reference_gpu"] = serve_reference_gpu(reqs, served["results"],
                                                           served["trials_per_s"])
