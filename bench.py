@@ -188,6 +188,52 @@ def _ref_process(path, N, dt, barrier, results):
     results.put(time.perf_counter() - t0)
 
 
+def _ref_one_thread(path, N, dt, results):
+    """The reference CPU path on one thread, in a process of its own that
+    loads the build whose FFT shim counts its transforms' time: (seconds of
+    the search, seconds in the FFT, FFT calls)."""
+    import ctypes as C
+    os.environ["CS_REF_LIBNAME"] = "libcsref_timed.so"
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import refbind as rb
+    from coherentsearch_c_b200.search import Options
+    amps = np.ascontiguousarray(np.load(path))
+    opts = Options(blocksize=BLOCKSIZE_CPU, threshold=8.0)
+    lib = rb.ref_lib()
+    lib.cs_shim_fft_seconds.argtypes = [C.POINTER(C.c_longlong), C.c_int]
+    lib.cs_shim_fft_seconds.restype = C.c_double
+    rb.pin_ref_threads(1)
+    calls = C.c_longlong(0)
+    lib.cs_shim_fft_seconds(C.byref(calls), 1)
+    t0 = time.perf_counter()
+    rb.ref_search(amps, N, dt, opts)
+    wall = time.perf_counter() - t0
+    fft = lib.cs_shim_fft_seconds(C.byref(calls), 1)
+    results.put((wall, fft, int(calls.value)))
+
+
+def _collect(queue, procs, n, timeout=600.0):
+    """n results from worker processes; an error if they all end (or the
+    time runs out) first.  The workers are joined, and ended if still
+    running, in every case."""
+    out = []
+    try:
+        deadline = time.perf_counter() + timeout
+        while len(out) < n:
+            try:
+                out.append(queue.get(timeout=1.0))
+            except Exception:   # noqa: BLE001  (queue.Empty)
+                if time.perf_counter() > deadline or not any(p.is_alive() for p in procs):
+                    raise RuntimeError(f"{n - len(out)} reference processes ended "
+                                       "without a result")
+    finally:
+        for p in procs:
+            p.join(timeout=10)
+            if p.is_alive():
+                p.terminate()
+    return out
+
+
 def cpu_reference_forms(amps, N, nproc=None):
     """The reference CPU path in its other two forms: one thread, and one
     single-threaded process per host core each searching the whole spectrum
@@ -196,47 +242,34 @@ def cpu_reference_forms(amps, N, nproc=None):
     Returns {"one_thread": ..., "processes": ...} in trials/s."""
     import multiprocessing as mp
     import tempfile
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import refbind as rb
     from coherentsearch_c_b200.search import Options
     dt = WORKLOAD["dt"]
     opts = Options(blocksize=BLOCKSIZE_CPU, threshold=8.0)
     _, _, total = opts.geometry(N, dt)
-    rb.ref_lib()
-    rb.pin_ref_threads(1)
-    t0 = time.perf_counter()
-    rb.ref_search(amps, N, dt, opts)
-    one = total / (time.perf_counter() - t0)
-    rb.pin_ref_threads(os.cpu_count() or 1)
     nproc = nproc or (os.cpu_count() or 1)
     ctx = mp.get_context("spawn")
     with tempfile.TemporaryDirectory() as tmp:
         path = os.path.join(tmp, "amps.npy")
         np.save(path, np.ascontiguousarray(amps))
+        q1 = ctx.Queue()
+        p1 = ctx.Process(target=_ref_one_thread, args=(path, N, dt, q1))
+        p1.start()
+        wall1, fft1, calls1 = _collect(q1, [p1], 1)[0]
+        one = total / wall1
         barrier = ctx.Barrier(nproc)
         results = ctx.Queue()
         procs = [ctx.Process(target=_ref_process, args=(path, N, dt, barrier, results))
                  for _ in range(nproc)]
         for p in procs:
             p.start()
-        times = []
-        try:
-            deadline = time.perf_counter() + 600.0
-            while len(times) < nproc:
-                try:
-                    times.append(results.get(timeout=1.0))
-                except Exception:   # noqa: BLE001  (queue.Empty)
-                    if (time.perf_counter() > deadline or
-                            not any(p.is_alive() for p in procs)):
-                        raise RuntimeError(f"{nproc - len(times)} reference processes "
-                                           "ended without a result")
-        finally:
-            for p in procs:
-                p.join(timeout=10)
-                if p.is_alive():
-                    p.terminate()
+        times = _collect(results, procs, nproc)
     return {"one_thread": {"value": one, "cores": 1,
-                           "sample": f"one full search ({total} trials), one OpenMP thread"},
+                           "sample": f"one full search ({total} trials), one OpenMP thread",
+                           # the FFT shim's share of the search, against the
+                           # reference README's single-thread split with FFTW
+                           # (base + decimated c2r 0.57 of 1.33 s)
+                           "fft_seconds": fft1, "fft_calls": calls1,
+                           "fft_share": fft1 / wall1, "fft_share_readme_fftw": 0.57 / 1.33},
             "processes": {"value": nproc * total / max(times), "cores": nproc,
                           "sample": f"{nproc} single-threaded processes, each one full search "
                                     f"({total} trials), started together; slowest "

@@ -499,8 +499,51 @@ static void shim_execute(struct cs_shim_plan *p)
     memcpy(p->out, tmp, (size_t)p->n * sizeof(cx_f));
 }
 
+#ifdef CS_SHIM_TIMING
+/* Time spent in the transforms, for the CPU baseline's phase split: built
+ * only into libcsref_timed.so.  Thread CPU time summed over the calls of the
+ * calling thread's process; meaningful with one OpenMP thread. */
+#include <time.h>
+static double g_fft_seconds;
+static long long g_fft_calls;
+
+static double thread_seconds(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_THREAD_CPUTIME_ID, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+static void shim_execute_timed(struct cs_shim_plan *p)
+{
+    const double t0 = thread_seconds();
+    shim_execute(p);
+    const double dt = thread_seconds() - t0;
+#pragma omp atomic
+    g_fft_seconds += dt;
+#pragma omp atomic
+    g_fft_calls += 1;
+}
+
+/* Seconds spent in fftw(f)_execute so far (and the number of calls);
+ * reset != 0 clears both after reading. */
+double cs_shim_fft_seconds(long long *calls, int reset)
+{
+    const double s = g_fft_seconds;
+    if (calls) *calls = g_fft_calls;
+    if (reset) {
+        g_fft_seconds = 0.0;
+        g_fft_calls = 0;
+    }
+    return s;
+}
+
+void fftw_execute(const fftw_plan p) { shim_execute_timed(p); }
+void fftwf_execute(const fftwf_plan p) { shim_execute_timed(p); }
+#else
 void fftw_execute(const fftw_plan p) { shim_execute(p); }
 void fftwf_execute(const fftwf_plan p) { shim_execute(p); }
+#endif
 
 static void shim_destroy(struct cs_shim_plan *p)
 {

@@ -50,7 +50,10 @@ def ref_lib() -> C.CDLL:
     global _REF
     if _REF is None:
         pin_ref_threads(1)
-        lib = nt.declare_host_api(C.CDLL(os.path.join(REF_DIR, "libcsref.so")))
+        # CS_REF_LIBNAME=libcsref_timed.so loads the build whose FFT shim
+        # counts the time spent in its transforms (cs_shim_fft_seconds)
+        name = os.environ.get("CS_REF_LIBNAME", "libcsref.so")
+        lib = nt.declare_host_api(C.CDLL(os.path.join(REF_DIR, name)))
         lib.datpipe_create.argtypes = [C.c_int, C.c_int, C.c_double]
         lib.datpipe_create.restype = C.c_void_p
         lib.datpipe_free.argtypes = [C.c_void_p]

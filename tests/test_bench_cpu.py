@@ -50,5 +50,8 @@ def test_cpu_reference_forms_run_and_report():
     amps = synth.amps_interleaved(synth.normalised_spectrum(x))
     forms = bench.cpu_reference_forms(amps, N, nproc=2)
     assert forms["one_thread"]["cores"] == 1 and forms["one_thread"]["value"] > 0
+    # the timed build of the reference: its FFT shim's share of the search
+    assert forms["one_thread"]["fft_calls"] > 0
+    assert 0.0 < forms["one_thread"]["fft_share"] < 1.0
     assert forms["processes"]["cores"] == 2 and forms["processes"]["value"] > 0
     assert "2 single-threaded processes" in forms["processes"]["sample"]
