@@ -59,6 +59,18 @@ KERNEL_NAMES = {0: "cs_search_kernel", 1: "search_ws_cfg60", 2: "search_f64",
                 3: "search_tma_cfg60", 4: "interp_tc + search_pre_cfg60"}
 
 
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), for the CPU baseline."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -419,7 +431,7 @@ def run_reference(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": WORKLOAD,
         "blocksize": BLOCKSIZE_CPU,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": sample},
+                         "sample": sample, "cpu_model": cpu_model()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -548,7 +560,8 @@ def run_b200(args):
         try:
             rate, cores, sample = cpu_reference_rate(amps, N, seconds=args.cpu_seconds)
             line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores,
-                                    "kind": "reference", "sample": sample}
+                                    "kind": "reference", "sample": sample,
+                                    "cpu_model": cpu_model()}
             try:
                 line["cpu_baseline"]["forms"] = cpu_reference_forms(amps, N)
             except Exception as exc:   # noqa: BLE001
