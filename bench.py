@@ -228,13 +228,14 @@ def _collect(queue, procs, n, timeout=600.0):
     """n results from worker processes; an error if they all end (or the
     time runs out) first.  The workers are joined, and ended if still
     running, in every case."""
+    import queue as queue_mod
     out = []
     try:
         deadline = time.perf_counter() + timeout
         while len(out) < n:
             try:
                 out.append(queue.get(timeout=1.0))
-            except Exception:   # noqa: BLE001  (queue.Empty)
+            except queue_mod.Empty:
                 if time.perf_counter() > deadline or not any(p.is_alive() for p in procs):
                     raise RuntimeError(f"{n - len(out)} reference processes ended "
                                        "without a result")
