@@ -60,3 +60,54 @@ def test_two_ranks_gather_in_list_order():
         assert p.exitcode == 0
     want = [r.tolist() for r in search_list(costs, fake_search, None)]
     assert got[0] == want and got[1] == want
+
+
+def failing_search(idx):
+    """A rank whose search fails before the gather (the host-side stand-in
+    for a replica that dies between steps)."""
+    raise RuntimeError("replica failed")
+
+
+def _worker_fault(rank, world, port, costs, out_q, mode):
+    import datetime
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    if mode == "never_joins" and rank == 1:
+        out_q.put((rank, "absent"))
+        return
+    try:
+        dist.init_process_group("gloo", rank=rank, world_size=world,
+                                timeout=datetime.timedelta(seconds=5))
+    except Exception as exc:   # noqa: BLE001
+        out_q.put((rank, f"error: {type(exc).__name__}"))
+        return
+    try:
+        fn = failing_search if (mode == "fails" and rank == 1) else fake_search
+        search_list(costs, fn, dist)
+        out_q.put((rank, "ok"))
+    except Exception as exc:   # noqa: BLE001
+        out_q.put((rank, f"error: {type(exc).__name__}"))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(120)
+@pytest.mark.parametrize("mode", ["fails", "never_joins"])
+def test_a_lost_rank_ends_the_others_with_an_error(mode):
+    """A rank that fails before the gather, or never joins, makes the other
+    rank's collective (or rendezvous) end with an error within the process
+    group's short timeout instead of waiting for good."""
+    costs = [float(c) for c in range(1, 12)]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker_fault, args=(r, 2, port, costs, q, mode))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=90) for _ in procs)
+    for p in procs:
+        p.join(timeout=30)
+        assert not p.is_alive()
+    assert got[0].startswith("error")
+    assert got[1] == ("absent" if mode == "never_joins" else "error: RuntimeError")
